@@ -1,0 +1,221 @@
+// Context, mesh and DOF-manager objects of the C ABI.
+#include <cstdio>
+
+#include "objects.h"
+
+namespace geo {
+
+void check_launch(geo_ctx* ctx, const char* what) {
+    (void)ctx;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) fail(GEO_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void sync(geo_ctx* ctx, const char* what) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) fail(GEO_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void reset_dev_err(geo_ctx* ctx) {
+    GEO_CUDA(cudaMemsetAsync(ctx->dev_err.p, 0, sizeof(int), ctx->stream));
+}
+
+int read_dev_err(geo_ctx* ctx) {
+    int h = 0;
+    GEO_CUDA(cudaMemcpyAsync(&h, ctx->dev_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx, "read device error word");
+    return h;
+}
+
+void raise_dev_err(geo_ctx* ctx, int bits, const char* what) {
+    if (bits & DEV_ERR_SINGULAR)
+        fail(GEO_ERR_SINGULAR_JACOBIAN, std::string(what) + ": Singular Jacobian");
+    if (bits & DEV_ERR_TIMEOUT)
+        fail(GEO_ERR_TIMEOUT, std::string(what) + ": device-side wait timed out");
+    if (bits & DEV_ERR_BOUNDS) fail(GEO_ERR_INVALID_ARG, std::string(what) + ": index out of range");
+    (void)ctx;
+}
+
+namespace {
+
+__global__ void aos_to_soa3(const double* __restrict__ aos, double* __restrict__ soa, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        soa[i] = aos[3 * i];
+        soa[n + i] = aos[3 * i + 1];
+        soa[2 * n + i] = aos[3 * i + 2];
+    }
+}
+
+__global__ void conn_to_soa(const int32_t* __restrict__ aos, int32_t* __restrict__ soa, int64_t E,
+                            int64_t n_nodes, int* err) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+         e += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int l = 0; l < 10; ++l) {
+            const int32_t v = aos[10 * e + l];
+            if (v < 0 || v >= n_nodes) atomicOr(err, DEV_ERR_BOUNDS);
+            soa[l * E + e] = v;
+        }
+    }
+}
+
+}  // namespace
+}  // namespace geo
+
+using namespace geo;
+
+extern "C" {
+
+const char* geo_version(void) { return "geofem-b200 0.1 (sm_100a)"; }
+
+int geo_device_count(int* count) {
+    GEO_API_BEGIN(nullptr)
+    GEO_CHECK_ARG(count, "count is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    GEO_API_END
+}
+
+int geo_ctx_create(int device, geo_ctx** out) {
+    GEO_API_BEGIN(nullptr)
+    GEO_CHECK_ARG(out, "out is NULL");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        fail(GEO_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    GEO_CHECK_ARG(device >= 0 && device < n, "device ordinal out of range");
+    GEO_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    GEO_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        fail(GEO_ERR_UNSUPPORTED, "libgeofem is built for sm_100a (B200); device is sm_" +
+                                      std::to_string(prop.major) + std::to_string(prop.minor));
+    auto ctx = std::make_unique<geo_ctx>();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    GEO_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    GEO_CUDA(cudaEventCreate(&ctx->ev0));
+    GEO_CUDA(cudaEventCreate(&ctx->ev1));
+    ctx->dev_err.alloc(4);
+    GEO_CUDA(cudaMemset(ctx->dev_err.p, 0, 4 * sizeof(int)));
+    *out = ctx.release();
+    GEO_API_END
+}
+
+int geo_ctx_destroy(geo_ctx* ctx) {
+    if (!ctx) return GEO_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->dev_err.release();
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return GEO_OK;
+}
+
+const char* geo_last_error(const geo_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : geo::g_thread_err.c_str();
+}
+
+int geo_sm_count(const geo_ctx* ctx, int* sm_count) {
+    if (!ctx || !sm_count) return GEO_ERR_INVALID_ARG;
+    *sm_count = ctx->sm_count;
+    return GEO_OK;
+}
+
+int geo_mesh_create(geo_ctx* ctx, int64_t n_nodes, const double* xyz, int64_t n_elem,
+                    const int32_t* conn, geo_mesh** out) {
+    GEO_API_BEGIN(ctx)
+    GEO_CHECK_ARG(ctx && out, "ctx/out is NULL");
+    GEO_CHECK_ARG(n_nodes > 0 && n_nodes < (int64_t(1) << 31), "n_nodes out of range");
+    GEO_CHECK_ARG(n_elem > 0 && n_elem * 10 < (int64_t(1) << 31), "n_elem out of range");
+    GEO_CHECK_ARG(xyz && conn, "xyz/conn is NULL");
+    auto m = std::make_unique<geo_mesh>();
+    m->ctx = ctx;
+    m->n_nodes = n_nodes;
+    m->n_elem = n_elem;
+    cudaStream_t s = ctx->stream;
+    // keep host copies for host-side operator set-up
+    m->h_xyz.resize(3 * n_nodes);
+    m->h_conn.resize(10 * n_elem);
+    GEO_CUDA(cudaMemcpyAsync(m->h_xyz.data(), xyz, 3 * n_nodes * sizeof(double), cudaMemcpyDefault, s));
+    GEO_CUDA(cudaMemcpyAsync(m->h_conn.data(), conn, 10 * n_elem * sizeof(int32_t), cudaMemcpyDefault, s));
+    DevBuf<double> txyz;
+    DevBuf<int32_t> tconn;
+    const double* dxyz = stage_in(xyz, 3 * n_nodes, txyz, s);
+    const int32_t* dconn = stage_in(conn, 10 * n_elem, tconn, s);
+    m->xyz.alloc(3 * n_nodes);
+    m->conn.alloc(10 * n_elem);
+    reset_dev_err(ctx);
+    aos_to_soa3<<<std::min<int64_t>(cdiv(n_nodes, 256), 65535), 256, 0, s>>>(dxyz, m->xyz.p, n_nodes);
+    check_launch(ctx, "aos_to_soa3");
+    conn_to_soa<<<std::min<int64_t>(cdiv(n_elem, 256), 65535), 256, 0, s>>>(dconn, m->conn.p, n_elem,
+                                                                             n_nodes, ctx->dev_err.p);
+    check_launch(ctx, "conn_to_soa");
+    const int bits = read_dev_err(ctx);
+    if (bits & DEV_ERR_BOUNDS) fail(GEO_ERR_INVALID_ARG, "connectivity references a node id out of range");
+    *out = m.release();
+    GEO_API_END
+}
+
+int geo_mesh_destroy(geo_mesh* mesh) {
+    if (!mesh) return GEO_OK;
+    cudaSetDevice(mesh->ctx->device);
+    delete mesh;
+    return GEO_OK;
+}
+
+int geo_dofs_create(geo_ctx* ctx, int64_t n_nodes, int32_t dofs_per_node, const uint8_t* mask,
+                    const double* values, geo_dofs** out) {
+    GEO_API_BEGIN(ctx)
+    GEO_CHECK_ARG(ctx && out, "ctx/out is NULL");
+    GEO_CHECK_ARG(n_nodes > 0, "n_nodes must be positive");
+    GEO_CHECK_ARG(dofs_per_node >= 1 && dofs_per_node <= 3, "dofs_per_node must be 1..3");
+    auto d = std::make_unique<geo_dofs>();
+    d->ctx = ctx;
+    d->n_nodes = n_nodes;
+    d->dpn = dofs_per_node;
+    d->n_dofs = n_nodes * dofs_per_node;
+    GEO_CHECK_ARG(d->n_dofs < (int64_t(1) << 31), "too many DOFs");
+    d->h_mask.assign(d->n_dofs, 0);
+    d->h_vals.assign(d->n_dofs, 0.0);
+    if (mask)
+        GEO_CUDA(cudaMemcpy(d->h_mask.data(), mask, d->n_dofs, cudaMemcpyDefault));
+    if (values)
+        GEO_CUDA(cudaMemcpy(d->h_vals.data(), values, d->n_dofs * sizeof(double), cudaMemcpyDefault));
+    int64_t nd = 0;
+    for (int64_t i = 0; i < d->n_dofs; ++i) {
+        d->h_mask[i] = d->h_mask[i] ? 1 : 0;
+        nd += d->h_mask[i];
+    }
+    d->n_dir = nd;
+    d->mask.alloc(d->n_dofs);
+    d->vals.alloc(d->n_dofs);
+    GEO_CUDA(cudaMemcpy(d->mask.p, d->h_mask.data(), d->n_dofs, cudaMemcpyHostToDevice));
+    GEO_CUDA(cudaMemcpy(d->vals.p, d->h_vals.data(), d->n_dofs * sizeof(double), cudaMemcpyHostToDevice));
+    *out = d.release();
+    GEO_API_END
+}
+
+int geo_dofs_num_dirichlet(const geo_dofs* dofs, int64_t* count) {
+    if (!dofs || !count) return GEO_ERR_INVALID_ARG;
+    *count = dofs->n_dir;
+    return GEO_OK;
+}
+
+int geo_dofs_destroy(geo_dofs* dofs) {
+    if (!dofs) return GEO_OK;
+    cudaSetDevice(dofs->ctx->device);
+    delete dofs;
+    return GEO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,222 @@
+// K4: FP64 Jacobi-PCG on an assembled CSR matrix, the drop-in for
+// ConjugateGradient::solve (linalg/iterative.rs:46-131) with
+// JacobiPreconditioner (linalg/preconditioner.rs:37-62).
+//
+// One persistent cooperative kernel runs the whole solve: sub-warp SpMV,
+// Jacobi scaling, axpys, and dot products reduced by warp shuffles into
+// per-block partials that every block sums in the same fixed order after a
+// bounded grid barrier (so all blocks take identical, deterministic decisions).
+#include "pcg_common.cuh"
+
+namespace geo {
+namespace {
+
+constexpr int kBS = 256;
+constexpr int kVec = 8;  // lanes per CSR row
+
+struct CsrPcgArgs {
+    const int64_t* indptr;
+    const int32_t* indices;
+    const double* data;
+    int64_t n;
+    const double* b;
+    double *x, *r, *p, *q, *dinv;
+    double *part_a, *part_b;
+    GridSync* gs;
+    PcgResult* res;
+    unsigned long long timeout_ns;
+    long long max_it;
+    double tol, abs_tol;
+    int use_prec;
+};
+
+__device__ __forceinline__ int64_t lower_bound_i32(const int32_t* idx, int64_t b, int64_t e, int32_t c) {
+    while (b < e) {
+        const int64_t m = (b + e) >> 1;
+        if (idx[m] < c) b = m + 1;
+        else e = m;
+    }
+    return b;
+}
+
+__global__ void __launch_bounds__(kBS) k_csr_pcg(CsrPcgArgs a) {
+    const unsigned nb = gridDim.x;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    const int64_t n = a.n;
+
+    // x = 0, r = b, z = M^-1 r, p = z (iterative.rs:70-75)
+    {
+        double v[2] = {0.0, 0.0};
+        for (int64_t i = tid; i < n; i += nth) {
+            double di = 1.0;
+            if (a.use_prec) {
+                const int64_t rb = a.indptr[i], re = a.indptr[i + 1];
+                const int64_t pp = lower_bound_i32(a.indices, rb, re, (int32_t)i);
+                if (pp < re && a.indices[pp] == i) {
+                    const double d = a.data[pp];
+                    if (fabs(d) > 1e-14) di = 1.0 / d;
+                }
+            }
+            a.dinv[i] = di;
+            const double bi = a.b[i];
+            const double zi = bi * di;
+            a.x[i] = 0.0;
+            a.r[i] = bi;
+            a.p[i] = zi;
+            v[0] += bi * bi;
+            v[1] += bi * zi;
+        }
+        store_partial<2>(a.part_b, v);
+    }
+    if (!grid_barrier(a.gs, nb, a.timeout_ns)) return;
+    double t2[2];
+    grid_total<2>(a.part_b, nb, t2);
+    const double bnorm = sqrt(t2[0]);
+    double rz = t2[1];
+    if (bnorm < 1e-25) {  // iterative.rs:60-68
+        if (tid == 0) *a.res = PcgResult{0, 0.0, bnorm, 1, 0, 0};
+        return;
+    }
+    long long it = 0;
+    int converged = 0, breakdown = 0;
+    double final_res = bnorm;
+    const int lane = threadIdx.x & 31, sub = lane % kVec;
+    const int64_t warp = tid >> 5, nwarps = nth >> 5;
+    constexpr int rows_per_warp = 32 / kVec;
+    while (it < a.max_it) {
+        // q = A p and p.q
+        {
+            double v[1] = {0.0};
+            for (int64_t rbase = warp * rows_per_warp; rbase < n; rbase += nwarps * rows_per_warp) {
+                const int64_t row = rbase + lane / kVec;
+                double s = 0.0;
+                if (row < n)
+                    for (int64_t pp = a.indptr[row] + sub; pp < a.indptr[row + 1]; pp += kVec)
+                        s += a.data[pp] * a.p[a.indices[pp]];
+#pragma unroll
+                for (int o = kVec / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, kVec);
+                if (row < n && sub == 0) {
+                    a.q[row] = s;
+                    v[0] += a.p[row] * s;
+                }
+            }
+            store_partial<1>(a.part_a, v);
+        }
+        if (!grid_barrier(a.gs, nb, a.timeout_ns)) return;
+        double pq[1];
+        grid_total<1>(a.part_a, nb, pq);
+        if (fabs(pq[0]) < 1e-30) {  // iterative.rs:85
+            breakdown = 1;
+            break;
+        }
+        const double alpha = rz / pq[0];
+        {
+            double v[2] = {0.0, 0.0};
+            for (int64_t i = tid; i < n; i += nth) {
+                const double pi = a.p[i];
+                a.x[i] += alpha * pi;
+                const double ri = a.r[i] - alpha * a.q[i];
+                a.r[i] = ri;
+                v[0] += ri * ri;
+                v[1] += ri * (ri * a.dinv[i]);
+            }
+            store_partial<2>(a.part_b, v);
+        }
+        if (!grid_barrier(a.gs, nb, a.timeout_ns)) return;
+        grid_total<2>(a.part_b, nb, t2);
+        const double rn = sqrt(t2[0]);
+        final_res = rn;
+        if (rn < a.tol * bnorm || rn < a.abs_tol) {  // iterative.rs:95
+            converged = 1;
+            break;
+        }
+        const double beta = t2[1] / rz;
+        rz = t2[1];
+        for (int64_t i = tid; i < n; i += nth) a.p[i] = a.r[i] * a.dinv[i] + beta * a.p[i];
+        if (!grid_barrier(a.gs, nb, a.timeout_ns)) return;
+        ++it;
+    }
+    if (tid == 0) *a.res = PcgResult{it, final_res, bnorm, converged, breakdown, 0};
+}
+
+}  // namespace
+}  // namespace geo
+
+using namespace geo;
+
+extern "C" {
+
+void geo_cg_opts_default(geo_cg_opts* o) {
+    if (!o) return;
+    o->max_iterations = 1000;
+    o->tolerance = 1e-8;
+    o->abs_tolerance = 1e-12;
+    o->use_preconditioner = 1;
+    o->precision = GEO_PRECISION_FP64;
+    o->reliable_delta = 0.1;
+    o->timeout_seconds = 10.0;
+}
+
+int geo_cg_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_opts* opts, double* x,
+                 geo_solver_stats* stats) {
+    GEO_API_BEGIN(ctx)
+    GEO_CHECK_ARG(ctx && A && b && x, "NULL argument");
+    GEO_CHECK_ARG(A->n_rows == A->n_cols, "matrix must be square");
+    geo_cg_opts o;
+    cg_opts_fill(opts, o);
+    GEO_CHECK_ARG(o.max_iterations >= 0, "max_iterations must be >= 0");
+    cudaStream_t s = ctx->stream;
+    const int64_t n = A->n_rows;
+    DevBuf<double> tb, work(5 * n);
+    const double* db = stage_in(b, n, tb, s);
+    const int nb = persistent_blocks(ctx, k_csr_pcg, kBS, 0);
+    PcgScratch sc;
+    sc.ensure(nb);
+    CsrPcgArgs args{};
+    args.indptr = A->indptr.p;
+    args.indices = A->indices.p;
+    args.data = A->data.p;
+    args.n = n;
+    args.b = db;
+    args.x = work.p;
+    args.r = work.p + n;
+    args.p = work.p + 2 * n;
+    args.q = work.p + 3 * n;
+    args.dinv = work.p + 4 * n;
+    args.part_a = sc.slot(0, nb);
+    args.part_b = sc.slot(1, nb);
+    args.gs = sc.gs.p;
+    args.res = sc.res.p;
+    args.timeout_ns = (unsigned long long)(o.timeout_seconds * 1e9);
+    args.max_it = o.max_iterations;
+    args.tol = o.tolerance;
+    args.abs_tol = o.abs_tolerance;
+    args.use_prec = o.use_preconditioner;
+    GEO_CUDA(cudaMemsetAsync(sc.gs.p, 0, sizeof(GridSync), s));
+    GEO_CUDA(cudaMemsetAsync(sc.res.p, 0, sizeof(PcgResult), s));
+    GEO_CUDA(cudaEventRecord(ctx->ev0, s));
+    launch_persistent(ctx, k_csr_pcg, kBS, 0, args, nb);
+    GEO_CUDA(cudaEventRecord(ctx->ev1, s));
+    PcgResult r{};
+    GridSync g{};
+    GEO_CUDA(cudaMemcpyAsync(&r, sc.res.p, sizeof(r), cudaMemcpyDeviceToHost, s));
+    GEO_CUDA(cudaMemcpyAsync(&g, sc.gs.p, sizeof(g), cudaMemcpyDeviceToHost, s));
+    copy_out(x, work.p, n, s);
+    sync(ctx, "geo_cg_solve");
+    float ms = 0.f;
+    GEO_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (g.error & DEV_ERR_TIMEOUT) {
+        fill_stats(stats, r, ms * 1e-3, GEO_ERR_TIMEOUT);
+        fail(GEO_ERR_TIMEOUT, "PCG grid barrier timed out");
+    }
+    const int status = r.converged ? GEO_OK : (r.breakdown ? GEO_ERR_BREAKDOWN : GEO_NOT_CONVERGED);
+    fill_stats(stats, r, ms * 1e-3, status);
+    if (status != GEO_OK) {
+        record_error(ctx, status, r.breakdown ? "CG breakdown: |p^T A p| < 1e-30" : "CG did not converge");
+        return status;
+    }
+    GEO_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,97 @@
+// Internal definitions of the opaque C-ABI objects and the cross-file helpers.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+struct geo_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    std::string err;
+    geo::DevBuf<int> dev_err;  // [0]: DEV_ERR_* bits of element kernels
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+struct geo_mesh {
+    geo_ctx* ctx = nullptr;
+    int64_t n_nodes = 0, n_elem = 0;
+    std::vector<double> h_xyz;     // AoS [N][3]
+    std::vector<int32_t> h_conn;   // AoS [E][10]
+    geo::DevBuf<double> xyz;       // SoA [3][N]
+    geo::DevBuf<int32_t> conn;     // SoA [10][E]
+    // node -> (element*10 + local) incidence list sorted by element (built lazily)
+    geo::DevBuf<int32_t> inc_ptr;  // [N+1]
+    geo::DevBuf<int32_t> inc;      // [E*10]
+    // node-level sparsity pattern (built lazily)
+    geo::DevBuf<int64_t> pat_ptr;  // [N+1]
+    geo::DevBuf<int32_t> pat_idx;  // [nnz]
+    int64_t pat_nnz = -1;
+};
+
+struct geo_dofs {
+    geo_ctx* ctx = nullptr;
+    int64_t n_nodes = 0, n_dofs = 0, n_dir = 0;
+    int dpn = 1;
+    std::vector<uint8_t> h_mask;
+    std::vector<double> h_vals;
+    geo::DevBuf<uint8_t> mask;
+    geo::DevBuf<double> vals;
+};
+
+struct geo_csr {
+    geo_ctx* ctx = nullptr;
+    int64_t n_rows = 0, n_cols = 0, nnz = 0;
+    geo::DevBuf<int64_t> indptr;
+    geo::DevBuf<int32_t> indices;
+    geo::DevBuf<double> data;
+};
+
+namespace geo {
+
+thread_local inline std::string g_thread_err;
+
+inline void record_error(geo_ctx* ctx, int code, const std::string& msg) {
+    (void)code;
+    if (ctx) ctx->err = msg;
+    g_thread_err = msg;
+}
+
+// Checks the launch, then the device error word written by element kernels.
+void check_launch(geo_ctx* ctx, const char* what);
+// Synchronises the context stream and raises on a CUDA error.
+void sync(geo_ctx* ctx, const char* what);
+// Clears / reads the context device error word.
+void reset_dev_err(geo_ctx* ctx);
+int read_dev_err(geo_ctx* ctx);
+void raise_dev_err(geo_ctx* ctx, int bits, const char* what);
+
+// assembly.cu
+void ensure_inverse_map(geo_mesh* m);
+void ensure_pattern(geo_mesh* m);
+
+}  // namespace geo
+
+#define GEO_API_BEGIN(ctxp)                                  \
+    geo_ctx* api_ctx_ = (ctxp);                              \
+    try {                                                    \
+        if (api_ctx_) GEO_CUDA(cudaSetDevice(api_ctx_->device));
+
+#define GEO_API_END                                                                  \
+    }                                                                                \
+    catch (const geo::Error& e) {                                                    \
+        geo::record_error(api_ctx_, e.code, e.msg);                                  \
+        return e.code;                                                               \
+    }                                                                                \
+    catch (const std::bad_alloc&) {                                                  \
+        geo::record_error(api_ctx_, GEO_ERR_OUT_OF_MEMORY, "host allocation failed"); \
+        return GEO_ERR_OUT_OF_MEMORY;                                                \
+    }                                                                                \
+    catch (const std::exception& ex) {                                               \
+        geo::record_error(api_ctx_, GEO_ERR_INVALID_ARG, ex.what());                 \
+        return GEO_ERR_INVALID_ARG;                                                  \
+    }                                                                                \
+    return GEO_OK;

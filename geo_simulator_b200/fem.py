@@ -1,0 +1,640 @@
+"""Host-side mirror of the reference's Tet10 hot-path API over the C ABI.
+
+Names, argument meaning and error behaviour follow msahamed/geo_simulator:
+
+* ``ImprovedMeshGenerator.generate_cube``   -- src/mesh_generator_improved.rs:19-169
+* ``Mesh``                                  -- src/mesh/geometry.rs:41-71
+* ``DofManager``                            -- src/fem/dof.rs:8-180
+* ``ElementMatrix`` / ``ElasticityElement`` / ``BodyForce`` -- src/fem/element.rs,
+  src/mechanics/{element,body_force}.rs (batched over every element of a mesh)
+* ``Assembler``                             -- src/fem/assembly.rs:22-239, 389-437, 906-937
+* ``ConjugateGradient`` / ``SolverStats``   -- src/linalg/iterative.rs:7-147, solver.rs:5-32
+* ``IsotropicElasticity``                   -- src/mechanics/constitutive.rs:15-102
+
+Every numeric call runs on the GPU through libgeofem.so; there is no CPU
+fallback. Arrays may be numpy (host) or torch CUDA tensors (device).
+Reference panics (singular Jacobian, wrong DOFs per node) raise ``GeoError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from ._native import GeoError
+
+__all__ = [
+    "Context", "Mesh", "ImprovedMeshGenerator", "DofManager", "IsotropicElasticity", "CsrMatrix",
+    "ElementMatrix", "ElasticityElement", "BodyForce", "Assembler", "SolverStats", "ConjugateGradient",
+    "ThermalOperator", "ElasticityOperator", "GeoError",
+]
+
+
+# --------------------------------------------------------------------------- plumbing
+def _ptr(a):
+    """Raw address of a numpy array or torch tensor (must be contiguous)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _f64(a):
+    if hasattr(a, "data_ptr") and not isinstance(a, np.ndarray):
+        import torch
+        if a.dtype != torch.float64:
+            raise TypeError("expected a float64 tensor")
+        return a.contiguous()
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One CUDA context/stream of libgeofem (geo_ctx)."""
+
+    _default: dict[int, "Context"] = {}
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        N.check(N.lib().geo_ctx_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    @classmethod
+    def default(cls, device: int = 0) -> "Context":
+        if device not in cls._default:
+            cls._default[device] = Context(device)
+        return cls._default[device]
+
+    def check(self, code, allow=()):
+        return N.check(code, self.h, allow)
+
+    def sm_count(self) -> int:
+        v = C.c_int()
+        self.check(N.lib().geo_sm_count(self.h, C.byref(v)))
+        return v.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                N.lib().geo_ctx_destroy(self.h)
+        except Exception:
+            pass
+
+
+def _ctx(ctx):
+    return ctx if ctx is not None else Context.default()
+
+
+# --------------------------------------------------------------------------- mesh
+class Mesh:
+    """Tet10 mesh: ``nodes`` float64 [N, 3], ``elements`` int32 [E, 10]."""
+
+    def __init__(self, nodes, elements):
+        self.nodes = np.ascontiguousarray(nodes, dtype=np.float64).reshape(-1, 3)
+        el = np.asarray(elements)
+        if el.size and (el.min() < 0 or el.max() >= self.nodes.shape[0]):
+            raise GeoError(N.GEO_ERR_INVALID_ARG, "element references a node id out of range")
+        self.elements = np.ascontiguousarray(el, dtype=np.int32).reshape(-1, 10)
+        self._handles = {}
+
+    def num_nodes(self) -> int:
+        return int(self.nodes.shape[0])
+
+    def num_elements(self) -> int:
+        return int(self.elements.shape[0])
+
+    def handle(self, ctx=None):
+        ctx = _ctx(ctx)
+        key = id(ctx)
+        if key not in self._handles:
+            h = C.c_void_p()
+            ctx.check(N.lib().geo_mesh_create(ctx.h, self.num_nodes(), _ptr(self.nodes), self.num_elements(),
+                                              _ptr(self.elements), C.byref(h)))
+            self._handles[key] = (ctx, h)
+        return self._handles[key][1]
+
+    def __del__(self):
+        for ctx, h in getattr(self, "_handles", {}).values():
+            try:
+                N.lib().geo_mesh_destroy(h)
+            except Exception:
+                pass
+
+
+class ImprovedMeshGenerator:
+    """mesh_generator_improved.rs:8-170 (6 tets per hex, shared edge midpoints)."""
+
+    @staticmethod
+    def generate_cube(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float) -> Mesh:
+        L = N.lib()
+        n_nodes, n_elem = C.c_int64(), C.c_int64()
+        N.check(L.geo_generate_cube_size(nx, ny, nz, C.byref(n_nodes), C.byref(n_elem)))
+        xyz = np.empty((n_nodes.value, 3), np.float64)
+        conn = np.empty((n_elem.value, 10), np.int32)
+        N.check(L.geo_generate_cube(nx, ny, nz, float(lx), float(ly), float(lz), _ptr(xyz), _ptr(conn)))
+        m = Mesh.__new__(Mesh)
+        m.nodes, m.elements, m._handles = xyz, conn, {}
+        return m
+
+
+# --------------------------------------------------------------------------- DOFs
+class DofManager:
+    """dof.rs:8-180 for a fixed number of DOFs per node (``new``, :37-50)."""
+
+    def __init__(self, num_nodes: int, dofs_per_node: int):
+        self._num_nodes = int(num_nodes)
+        self._dpn = int(dofs_per_node)
+        self._mask = np.zeros(self._num_nodes * self._dpn, np.uint8)
+        self._values = np.zeros(self._num_nodes * self._dpn, np.float64)
+        self._handles = {}
+
+    # dof.rs:87-106
+    def global_dof(self, node_id: int, local_dof: int) -> int:
+        if local_dof >= self._dpn:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, "Node has no pressure DOF")
+        return node_id * self._dpn + local_dof
+
+    velocity_dof = global_dof
+
+    # dof.rs:113-130
+    def set_dirichlet(self, dof, value):
+        self._mask[dof] = 1
+        self._values[dof] = value
+        self._handles.clear()
+
+    def set_dirichlet_node(self, node_id, value):
+        for c in range(self._dpn):
+            self.set_dirichlet(np.asarray(node_id) * self._dpn + c, value)
+
+    def is_dirichlet(self, dof) -> bool:
+        return bool(self._mask[dof])
+
+    def get_dirichlet_value(self, dof) -> float:
+        return float(self._values[dof])
+
+    def total_dofs(self) -> int:
+        return self._num_nodes * self._dpn
+
+    def num_free_dofs(self) -> int:
+        return self.total_dofs() - int(self._mask.sum())
+
+    def num_constrained_dofs(self) -> int:
+        return int(self._mask.sum())
+
+    def dofs_per_node(self) -> int:
+        return self._dpn
+
+    def num_nodes(self) -> int:
+        return self._num_nodes
+
+    @property
+    def dirichlet_mask(self):
+        return self._mask
+
+    @property
+    def dirichlet_values(self):
+        return self._values
+
+    def handle(self, ctx=None):
+        ctx = _ctx(ctx)
+        key = id(ctx)
+        if key not in self._handles:
+            h = C.c_void_p()
+            ctx.check(N.lib().geo_dofs_create(ctx.h, self._num_nodes, self._dpn, _ptr(self._mask),
+                                              _ptr(self._values), C.byref(h)))
+            self._handles[key] = _DofsHandle(h)
+        return self._handles[key].h
+
+
+class _DofsHandle:
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self):
+        try:
+            N.lib().geo_dofs_destroy(self.h)
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------- material
+@dataclass
+class IsotropicElasticity:
+    """constitutive.rs:15-41 (E > 0, -1 < nu < 0.5)."""
+    youngs_modulus: float
+    poisson_ratio: float
+
+    def __post_init__(self):
+        if not self.youngs_modulus > 0.0:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, "Young's modulus must be positive")
+        if not (-1.0 < self.poisson_ratio < 0.5):
+            raise GeoError(N.GEO_ERR_INVALID_ARG, "Poisson's ratio must be in (-1, 0.5) for physical stability")
+
+    @staticmethod
+    def new(youngs_modulus, poisson_ratio):
+        return IsotropicElasticity(youngs_modulus, poisson_ratio)
+
+
+# --------------------------------------------------------------------------- CSR
+class CsrMatrix:
+    """Device-resident CSR (the sprs CsMat<f64> the reference returns)."""
+
+    def __init__(self, h, ctx):
+        self.h, self.ctx = h, ctx
+        r, c, z = C.c_int64(), C.c_int64(), C.c_int64()
+        N.check(N.lib().geo_csr_info(h, C.byref(r), C.byref(c), C.byref(z)))
+        self._shape = (r.value, c.value)
+        self._nnz = z.value
+
+    @classmethod
+    def from_arrays(cls, n_rows, n_cols, indptr, indices, data, ctx=None):
+        ctx = _ctx(ctx)
+        indptr = np.ascontiguousarray(indptr, np.int64)
+        indices = np.ascontiguousarray(indices, np.int32)
+        data = np.ascontiguousarray(data, np.float64)
+        h = C.c_void_p()
+        ctx.check(N.lib().geo_csr_create(ctx.h, n_rows, n_cols, indices.size, _ptr(indptr), _ptr(indices),
+                                         _ptr(data), C.byref(h)))
+        return cls(h, ctx)
+
+    @classmethod
+    def from_triplets(cls, n_rows, n_cols, rows, cols, vals, ctx=None):
+        """TriMat::add_triplet + to_csr (duplicates summed, explicit zeros kept)."""
+        rows, cols = np.asarray(rows, np.int64), np.asarray(cols, np.int64)
+        vals = np.asarray(vals, np.float64)
+        order = np.lexsort((cols, rows))
+        r, c, v = rows[order], cols[order], vals[order]
+        key = r * n_cols + c
+        uniq, start = np.unique(key, return_index=True)
+        data = np.add.reduceat(v, start) if v.size else v
+        ur, uc = uniq // n_cols, uniq % n_cols
+        indptr = np.zeros(n_rows + 1, np.int64)
+        np.add.at(indptr, ur + 1, 1)
+        return cls.from_arrays(n_rows, n_cols, np.cumsum(indptr), uc, data, ctx)
+
+    def rows(self):
+        return self._shape[0]
+
+    def cols(self):
+        return self._shape[1]
+
+    def nnz(self):
+        return self._nnz
+
+    @property
+    def shape(self):
+        return self._shape
+
+    def to_host(self):
+        ip = np.empty(self._shape[0] + 1, np.int64)
+        ix = np.empty(self._nnz, np.int32)
+        d = np.empty(self._nnz, np.float64)
+        self.ctx.check(N.lib().geo_csr_copy(self.h, _ptr(ip), _ptr(ix), _ptr(d)))
+        return ip, ix, d
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        ip, ix, d = self.to_host()
+        return sp.csr_matrix((d, ix, ip), shape=self._shape)
+
+    def apply(self, x):
+        """LinearOperator::apply (solver.rs:61-73)."""
+        x = _f64(x)
+        y = np.empty(self._shape[0]) if isinstance(x, np.ndarray) else x.new_empty(self._shape[0])
+        self.ctx.check(N.lib().geo_csr_apply(self.ctx.h, self.h, _ptr(x), _ptr(y)))
+        return y
+
+    def __del__(self):
+        try:
+            N.lib().geo_csr_destroy(self.h)
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------- elements
+def _coef_ptr(coef, n_elem):
+    if np.isscalar(coef):
+        return None, float(coef), None
+    a = _f64(coef)
+    if a.shape[0] != n_elem:
+        raise GeoError(N.GEO_ERR_INVALID_ARG, "per-element coefficient array has the wrong length")
+    return _ptr(a), 0.0, a
+
+
+class ElementMatrix:
+    """element.rs:8-140, batched: one matrix per element of ``mesh``."""
+
+    @staticmethod
+    def thermal_stiffness(mesh: Mesh, conductivity, ctx=None):
+        ctx = _ctx(ctx)
+        p, k, keep = _coef_ptr(conductivity, mesh.num_elements())
+        out = np.empty((mesh.num_elements(), 10, 10))
+        ctx.check(N.lib().geo_element_thermal_stiffness(ctx.h, mesh.handle(ctx), p, k, _ptr(out)))
+        return out
+
+    @staticmethod
+    def thermal_mass(mesh: Mesh, density, specific_heat, ctx=None):
+        ctx = _ctx(ctx)
+        out = np.empty((mesh.num_elements(), 10, 10))
+        ctx.check(N.lib().geo_element_thermal_mass(ctx.h, mesh.handle(ctx), float(density),
+                                                   float(specific_heat), _ptr(out)))
+        return out
+
+    @staticmethod
+    def thermal_load(mesh: Mesh, source, ctx=None):
+        ctx = _ctx(ctx)
+        out = np.empty((mesh.num_elements(), 10))
+        ctx.check(N.lib().geo_element_thermal_load(ctx.h, mesh.handle(ctx), float(source), _ptr(out)))
+        return out
+
+
+class ElasticityElement:
+    """mechanics/element.rs:33-65, batched."""
+
+    @staticmethod
+    def stiffness_matrix(mesh: Mesh, material: IsotropicElasticity, youngs_e=None, ctx=None):
+        ctx = _ctx(ctx)
+        ee = None if youngs_e is None else _f64(youngs_e)
+        out = np.empty((mesh.num_elements(), 30, 30))
+        ctx.check(N.lib().geo_element_elasticity_stiffness(ctx.h, mesh.handle(ctx), _ptr(ee),
+                                                           float(material.youngs_modulus),
+                                                           float(material.poisson_ratio), _ptr(out)))
+        return out
+
+
+class BodyForce:
+    """mechanics/body_force.rs:49-84, batched."""
+
+    @staticmethod
+    def gravity_load(mesh: Mesh, density, gravity, ctx=None):
+        ctx = _ctx(ctx)
+        g = np.ascontiguousarray(gravity, np.float64)
+        out = np.empty((mesh.num_elements(), 30))
+        ctx.check(N.lib().geo_element_gravity_load(ctx.h, mesh.handle(ctx), float(density), _ptr(g), _ptr(out)))
+        return out
+
+
+# --------------------------------------------------------------------------- assembly
+class Assembler:
+    """assembly.rs:7-1021 (the hot-path subset)."""
+
+    @staticmethod
+    def assemble_thermal_stiffness_parallel(mesh: Mesh, dof_mgr: DofManager, conductivity, ctx=None):
+        ctx = _ctx(ctx)
+        p, k, keep = _coef_ptr(conductivity, mesh.num_elements())
+        h = C.c_void_p()
+        ctx.check(N.lib().geo_assemble_thermal_stiffness(ctx.h, mesh.handle(ctx), dof_mgr.handle(ctx), p, k,
+                                                         C.byref(h)))
+        return CsrMatrix(h, ctx)
+
+    # the serial variant has the same result (assembly.rs:22-58)
+    assemble_thermal_stiffness_serial = assemble_thermal_stiffness_parallel
+
+    @staticmethod
+    def assemble_thermal_load(mesh: Mesh, dof_mgr: DofManager, source, ctx=None):
+        ctx = _ctx(ctx)
+        f = np.empty(dof_mgr.total_dofs())
+        ctx.check(N.lib().geo_assemble_thermal_load(ctx.h, mesh.handle(ctx), dof_mgr.handle(ctx), float(source),
+                                                    _ptr(f)))
+        return f
+
+    @staticmethod
+    def apply_dirichlet_bcs(K: CsrMatrix, f, dof_mgr: DofManager, ctx=None):
+        ctx = ctx or K.ctx
+        f = _f64(f)
+        h = C.c_void_p()
+        fbc = np.empty(K.rows())
+        ctx.check(N.lib().geo_apply_dirichlet_bcs(ctx.h, K.h, _ptr(f), dof_mgr.handle(ctx), C.byref(h), _ptr(fbc)))
+        return CsrMatrix(h, ctx), fbc
+
+    @staticmethod
+    def apply_dirichlet_bcs_only_matrix(K: CsrMatrix, dof_mgr: DofManager, ctx=None):
+        return Assembler.apply_dirichlet_bcs(K, np.zeros(K.rows()), dof_mgr, ctx)[0]
+
+    @staticmethod
+    def assemble_elasticity_stiffness_parallel(mesh: Mesh, dof_mgr: DofManager, material: IsotropicElasticity,
+                                               youngs_e=None, ctx=None):
+        ctx = _ctx(ctx)
+        ee = None if youngs_e is None else _f64(youngs_e)
+        h = C.c_void_p()
+        ctx.check(N.lib().geo_assemble_elasticity_stiffness(ctx.h, mesh.handle(ctx), dof_mgr.handle(ctx),
+                                                            _ptr(ee), float(material.youngs_modulus),
+                                                            float(material.poisson_ratio), C.byref(h)))
+        return CsrMatrix(h, ctx)
+
+    assemble_elasticity_stiffness_serial = assemble_elasticity_stiffness_parallel
+
+    @staticmethod
+    def assemble_gravity_load(mesh: Mesh, dof_mgr: DofManager, density, gravity, ctx=None):
+        ctx = _ctx(ctx)
+        g = np.ascontiguousarray(gravity, np.float64)
+        f = np.empty(dof_mgr.total_dofs())
+        ctx.check(N.lib().geo_assemble_gravity_load(ctx.h, mesh.handle(ctx), dof_mgr.handle(ctx), float(density),
+                                                    _ptr(g), _ptr(f)))
+        return f
+
+
+# --------------------------------------------------------------------------- solvers
+@dataclass
+class SolverStats:
+    """solver.rs:5-20 plus extensions."""
+    iterations: int = 0
+    residual_norm: float = 0.0
+    relative_residual: float = 0.0
+    converged: bool = False
+    solve_time: float = 0.0
+    status: int = 0
+    fp64_residual_updates: int = 0
+    b_norm: float = 0.0
+
+    @classmethod
+    def from_c(cls, s: N.SolverStatsC):
+        return cls(int(s.iterations), float(s.residual_norm), float(s.relative_residual), bool(s.converged),
+                   float(s.solve_time), int(s.status), int(s.fp64_residual_updates), float(s.b_norm))
+
+
+class ConjugateGradient:
+    """iterative.rs:7-147: Jacobi-preconditioned CG with the builder API."""
+
+    def __init__(self):
+        self.max_iterations = 1000
+        self.tolerance = 1e-8
+        self.abs_tolerance = 1e-12
+        self.use_preconditioner = True
+        self.precision = N.PRECISION_FP64
+        self.reliable_delta = 0.1
+        self.timeout_seconds = 10.0
+        self.name = "ConjugateGradient"
+
+    @staticmethod
+    def new():
+        return ConjugateGradient()
+
+    def with_max_iterations(self, n):
+        self.max_iterations = int(n)
+        return self
+
+    def with_tolerance(self, t):
+        self.tolerance = float(t)
+        return self
+
+    def with_abs_tolerance(self, t):
+        self.abs_tolerance = float(t)
+        return self
+
+    def with_preconditioner(self, flag):
+        self.use_preconditioner = bool(flag)
+        return self
+
+    def with_precision(self, precision):
+        """'fp64' (default, the reference semantics) or 'mixed' (matrix-free only)."""
+        self.precision = {"fp64": N.PRECISION_FP64, "mixed": N.PRECISION_MIXED}.get(precision, precision)
+        return self
+
+    def opts(self) -> N.CgOpts:
+        o = N.default_opts()
+        o.max_iterations = self.max_iterations
+        o.tolerance = self.tolerance
+        o.abs_tolerance = self.abs_tolerance
+        o.use_preconditioner = int(self.use_preconditioner)
+        o.precision = int(self.precision)
+        o.reliable_delta = self.reliable_delta
+        o.timeout_seconds = self.timeout_seconds
+        return o
+
+    def solve(self, A: CsrMatrix, b):
+        """Solver::solve (iterative.rs:123-131). Returns (x, SolverStats)."""
+        b = _f64(b)
+        x = np.empty(A.rows()) if isinstance(b, np.ndarray) else b.new_empty(A.rows())
+        st = N.SolverStatsC()
+        o = self.opts()
+        A.ctx.check(N.lib().geo_cg_solve(A.ctx.h, A.h, _ptr(b), C.byref(o), _ptr(x), C.byref(st)),
+                    allow=(N.GEO_NOT_CONVERGED, N.GEO_ERR_BREAKDOWN))
+        return x, SolverStats.from_c(st)
+
+    def solve_with_operator(self, op: "_MatFreeOperator", b):
+        """Solver::solve_with_operator (solver.rs:112-120) for a matrix-free operator."""
+        return op.solve(b, self)
+
+
+# --------------------------------------------------------------------------- matrix-free
+class _MatFreeOperator:
+    _create = None
+
+    def _init(self, mesh, dof_mgr, ctx, h):
+        self.mesh, self.dof_mgr, self.ctx, self.h = mesh, dof_mgr, ctx, h
+        nd, ne, cd = C.c_int64(), C.c_int64(), C.c_double()
+        N.check(N.lib().geo_op_info(h, C.byref(nd), C.byref(ne), C.byref(cd)))
+        self.n_dofs, self.n_elem, self.char_diag = nd.value, ne.value, cd.value
+
+    def rows(self):
+        return self.n_dofs
+
+    cols = rows
+
+    def _out(self, like, n):
+        return np.empty(n) if isinstance(like, np.ndarray) else like.new_empty(n)
+
+    def set_coefficients(self, coef):
+        p, k, keep = _coef_ptr(coef, self.n_elem)
+        self.ctx.check(N.lib().geo_op_set_coefficients(self.h, p, k))
+        cd = C.c_double()
+        N.check(N.lib().geo_op_info(self.h, None, None, C.byref(cd)))
+        self.char_diag = cd.value
+
+    def apply(self, x, precision="fp64"):
+        x = _f64(x)
+        y = self._out(x, self.n_dofs)
+        prec = N.PRECISION_MIXED if precision == "mixed" else N.PRECISION_FP64
+        self.ctx.check(N.lib().geo_op_apply(self.h, _ptr(x), _ptr(y), prec))
+        return y
+
+    def lift_rhs(self, f):
+        f = _f64(f)
+        out = self._out(f, self.n_dofs)
+        self.ctx.check(N.lib().geo_op_lift_rhs(self.h, _ptr(f), _ptr(out)))
+        return out
+
+    def diagonal(self):
+        d = np.empty(self.n_dofs)
+        self.ctx.check(N.lib().geo_op_diagonal(self.h, _ptr(d)))
+        return d
+
+    def solve(self, b, solver: ConjugateGradient | None = None):
+        solver = solver or ConjugateGradient()
+        b = _f64(b)
+        x = self._out(b, self.n_dofs)
+        st = N.SolverStatsC()
+        o = solver.opts()
+        self.ctx.check(N.lib().geo_cg_solve_matfree(self.h, _ptr(b), C.byref(o), _ptr(x), C.byref(st)),
+                       allow=(N.GEO_NOT_CONVERGED, N.GEO_ERR_BREAKDOWN))
+        return x, SolverStats.from_c(st)
+
+    def forward(self, f, solver: ConjugateGradient | None = None):
+        solver = solver or ConjugateGradient()
+        f = _f64(f)
+        u = self._out(f, self.n_dofs)
+        st = N.SolverStatsC()
+        o = solver.opts()
+        self.ctx.check(N.lib().geo_forward(self.h, _ptr(f), C.byref(o), _ptr(u), C.byref(st)),
+                       allow=(N.GEO_NOT_CONVERGED,))
+        return u, SolverStats.from_c(st)
+
+    def vjp(self, dJ_du, u=None, f=None, solver: ConjugateGradient | None = None):
+        """dJ/d(ln coef_e) given dJ/du; u=None recomputes the forward solution from f."""
+        solver = solver or ConjugateGradient()
+        g = _f64(dJ_du)
+        out = self._out(g, self.n_elem)
+        st = N.SolverStatsC()
+        o = solver.opts()
+        uu = None if u is None else _f64(u)
+        ff = None if f is None else _f64(f)
+        self.ctx.check(N.lib().geo_vjp(self.h, _ptr(ff), _ptr(uu), _ptr(g), C.byref(o), _ptr(out), C.byref(st)),
+                       allow=(N.GEO_NOT_CONVERGED,))
+        return out, SolverStats.from_c(st)
+
+    def element_gradient(self, u, lam):
+        u, lam = _f64(u), _f64(lam)
+        out = self._out(u, self.n_elem)
+        self.ctx.check(N.lib().geo_op_element_gradient(self.h, _ptr(u), _ptr(lam), _ptr(out)))
+        return out
+
+    def __del__(self):
+        try:
+            N.lib().geo_op_destroy(self.h)
+        except Exception:
+            pass
+
+
+class ThermalOperator(_MatFreeOperator):
+    """Matrix-free K_bc of apply_dirichlet_bcs(assemble_thermal_stiffness_parallel(..))."""
+
+    def __init__(self, mesh: Mesh, dof_mgr: DofManager, conductivity, ctx=None):
+        ctx = _ctx(ctx)
+        p, k, keep = _coef_ptr(conductivity, mesh.num_elements())
+        h = C.c_void_p()
+        ctx.check(N.lib().geo_thermal_operator_create(ctx.h, mesh.handle(ctx), dof_mgr.handle(ctx), p, k,
+                                                      C.byref(h)))
+        self._init(mesh, dof_mgr, ctx, h)
+
+
+class ElasticityOperator(_MatFreeOperator):
+    """Matrix-free K_bc of the 3-DOF elasticity system (assembly.rs:389-437 + :168-230)."""
+
+    def __init__(self, mesh: Mesh, dof_mgr: DofManager, material: IsotropicElasticity, youngs_e=None, ctx=None):
+        ctx = _ctx(ctx)
+        ee = None if youngs_e is None else _f64(youngs_e)
+        h = C.c_void_p()
+        ctx.check(N.lib().geo_elasticity_operator_create(ctx.h, mesh.handle(ctx), dof_mgr.handle(ctx), _ptr(ee),
+                                                         float(material.youngs_modulus),
+                                                         float(material.poisson_ratio), C.byref(h)))
+        self._init(mesh, dof_mgr, ctx, h)

@@ -1,0 +1,230 @@
+/*
+ * geo_fem.h -- C ABI of the B200 (sm_100a) Tet10 FEM hot path.
+ *
+ * Drop-in for the Rust hot path of msahamed/geo_simulator:
+ *   src/fem/element.rs, src/fem/assembly.rs, src/mechanics/*, src/linalg/{solver,
+ *   iterative,preconditioner}.rs.
+ * Each entry point names the reference item it replaces (file:line inside the
+ * reference project). A Rust crate binds these with `extern "C"`; the
+ * Python host package (geo_simulator_b200) and include/geofem.hpp bind them too.
+ *
+ * Conventions
+ *  - Every call returns an int status (GEO_OK = 0). Panics of the reference
+ *    (singular Jacobian, wrong DOFs per node, failed LU) become error codes;
+ *    geo_last_error(ctx) gives the message. Non-convergence is GEO_NOT_CONVERGED
+ *    with the solution and statistics still written (the reference reports it
+ *    in SolverStats.converged only).
+ *  - Pointer arguments to numeric arrays may be host memory (pageable or pinned)
+ *    or device memory of the context's GPU: the library checks each pointer and
+ *    copies host data in/out itself. All work runs on the context's stream and
+ *    every call synchronises before it returns.
+ *  - Objects (mesh, dofs, csr, op) are owned by the caller and freed with the
+ *    matching *_destroy. One context per host thread; calls on one context are
+ *    not re-entrant.
+ *  - Indices: connectivity and CSR column indices are int32 (the reference uses
+ *    usize); node and DOF counts must stay below 2^31. CSR row pointers are int64.
+ *  - Layouts follow the reference: coordinates AoS [n_nodes][3] double,
+ *    connectivity [n_elem][10] with the Tet10 local order
+ *    [v0 v1 v2 v3 e01 e12 e20 e03 e13 e23] (src/mesh/topology.rs:1-16),
+ *    DOF numbering dof = node * dofs_per_node + component (src/fem/dof.rs:87-91).
+ */
+#ifndef GEO_FEM_H
+#define GEO_FEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define GEO_OK 0
+#define GEO_ERR_INVALID_ARG 1
+#define GEO_ERR_SINGULAR_JACOBIAN 2 /* basis.rs:247 `expect("Singular Jacobian")` */
+#define GEO_NOT_CONVERGED 3         /* x and stats valid, stats.converged == 0   */
+#define GEO_ERR_BREAKDOWN 4         /* |p^T A p| < 1e-30 (iterative.rs:85); x valid */
+#define GEO_ERR_TIMEOUT 5           /* a bounded device-side wait ran out        */
+#define GEO_ERR_CUDA 6
+#define GEO_ERR_UNSUPPORTED 7
+#define GEO_ERR_NO_DEVICE 8
+#define GEO_ERR_OUT_OF_MEMORY 9
+
+/* precision of the matrix-free solver (geo_cg_opts.precision) */
+#define GEO_PRECISION_FP64 0  /* plain FP64 throughout (the drop-in semantics)           */
+#define GEO_PRECISION_MIXED 1 /* FP32 apply + FP32 PCG, FP64 residual refresh and update */
+
+typedef struct geo_ctx geo_ctx;
+typedef struct geo_mesh geo_mesh;
+typedef struct geo_dofs geo_dofs;
+typedef struct geo_csr geo_csr;
+typedef struct geo_op geo_op;
+
+/* ConjugateGradient builder state, iterative.rs:7-44 (defaults :16-24). */
+typedef struct geo_cg_opts {
+    int64_t max_iterations;     /* with_max_iterations, default 1000  */
+    double tolerance;           /* with_tolerance, default 1e-8       */
+    double abs_tolerance;       /* with_abs_tolerance, default 1e-12  */
+    int32_t use_preconditioner; /* with_preconditioner, default 1 (Jacobi) */
+    int32_t precision;          /* matrix-free only: GEO_PRECISION_*, default FP64 */
+    double reliable_delta;      /* MIXED: refresh the FP64 residual each time the FP32
+                                   residual drops by this factor (default 0.1) */
+    double timeout_seconds;     /* bound on every device-side grid barrier (default 10) */
+} geo_cg_opts;
+
+/* SolverStats, linalg/solver.rs:5-20, field by field, plus extensions. */
+typedef struct geo_solver_stats {
+    int64_t iterations;       /* completed PCG iterations (iterative.rs:81-110 counting) */
+    double residual_norm;     /* FP64: last recursive ||r||; MIXED: last true ||b - A x|| */
+    double relative_residual; /* residual_norm / ||b|| (0 if ||b|| <= 1e-20)       */
+    int32_t converged;
+    double solve_time;        /* seconds, CUDA events around the device work       */
+    /* extensions */
+    int32_t status;                 /* GEO_* code of the solve                      */
+    int64_t fp64_residual_updates;  /* MIXED: number of FP64 residual refreshes     */
+    double b_norm;
+    double kernel_time;             /* seconds inside the persistent PCG kernel     */
+} geo_solver_stats;
+
+/* ------------------------------------------------------------------ context */
+int geo_device_count(int* count);
+int geo_ctx_create(int device, geo_ctx** out);
+int geo_ctx_destroy(geo_ctx* ctx);
+const char* geo_last_error(const geo_ctx* ctx);
+const char* geo_version(void);
+int geo_sm_count(const geo_ctx* ctx, int* sm_count);
+
+/* ------------------------------------------------------------------ mesh */
+/* ImprovedMeshGenerator::generate_cube, mesh_generator_improved.rs:19-169 (host
+ * code, bit-exact node numbering and connectivity). geo_generate_cube_size gives
+ * the array sizes; xyz is [n_nodes][3], conn is [n_elem][10] (host memory).     */
+int geo_generate_cube_size(int64_t nx, int64_t ny, int64_t nz, int64_t* n_nodes, int64_t* n_elem);
+int geo_generate_cube(int64_t nx, int64_t ny, int64_t nz, double lx, double ly, double lz,
+                      double* xyz, int32_t* conn);
+
+/* Mesh{geometry.nodes, connectivity.tet10_elements}, mesh/geometry.rs:41-71.
+ * Uploaded once; the device keeps SoA coordinates and SoA connectivity.       */
+int geo_mesh_create(geo_ctx* ctx, int64_t n_nodes, const double* xyz, int64_t n_elem,
+                    const int32_t* conn, geo_mesh** out);
+int geo_mesh_destroy(geo_mesh* mesh);
+
+/* DofManager::new + set_dirichlet, dof.rs:37-50, :113-130. dirichlet_mask[n_dofs]
+ * (nonzero = constrained) and dirichlet_values[n_dofs]; either may be NULL.     */
+int geo_dofs_create(geo_ctx* ctx, int64_t n_nodes, int32_t dofs_per_node,
+                    const uint8_t* dirichlet_mask, const double* dirichlet_values, geo_dofs** out);
+int geo_dofs_num_dirichlet(const geo_dofs* dofs, int64_t* count);
+int geo_dofs_destroy(geo_dofs* dofs);
+
+/* ------------------------------------------------------------------ K1: element integration */
+/* Per-element matrices for every element of the mesh, row-major per element.
+ * k_e / E_e: per-element coefficient array, or NULL for the uniform scalar.   */
+/* ElementMatrix::thermal_stiffness, element.rs:23-61 (4-point rule): ke[n_elem][10][10] */
+int geo_element_thermal_stiffness(geo_ctx* ctx, const geo_mesh* mesh, const double* k_e, double k,
+                                  double* ke);
+/* ElementMatrix::thermal_mass, element.rs:74-105 (5-point rule): me[n_elem][10][10] */
+int geo_element_thermal_mass(geo_ctx* ctx, const geo_mesh* mesh, double density,
+                             double specific_heat, double* me);
+/* ElementMatrix::thermal_load, element.rs:117-140: fe[n_elem][10] */
+int geo_element_thermal_load(geo_ctx* ctx, const geo_mesh* mesh, double source, double* fe);
+/* ElasticityElement::stiffness_matrix, mechanics/element.rs:33-65 with
+ * IsotropicElasticity::constitutive_matrix, mechanics/constitutive.rs:63-102:
+ * ke[n_elem][30][30] */
+int geo_element_elasticity_stiffness(geo_ctx* ctx, const geo_mesh* mesh, const double* E_e,
+                                     double E, double nu, double* ke);
+/* BodyForce::gravity_load, mechanics/body_force.rs:49-84: fe[n_elem][30] */
+int geo_element_gravity_load(geo_ctx* ctx, const geo_mesh* mesh, double density,
+                             const double gravity[3], double* fe);
+
+/* ------------------------------------------------------------------ K2/K3: CSR assembly */
+/* Assembler::assemble_thermal_stiffness_parallel, assembly.rs:69-117. Rows and
+ * columns are node ids (dofs must have 1 DOF per node). Structure bit-exact with
+ * sprs TriMat::to_csr: sorted columns, duplicates summed (in element order),
+ * every structural entry kept.                                                 */
+int geo_assemble_thermal_stiffness(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs,
+                                   const double* k_e, double k, geo_csr** K);
+/* Assembler::assemble_thermal_load, assembly.rs:130-154: f[n_dofs] */
+int geo_assemble_thermal_load(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs,
+                              double source, double* f);
+/* Assembler::apply_dirichlet_bcs, assembly.rs:168-230: char_diag = max(1, max|K_ii|);
+ * free rows: f_i -= sum_{j in D} K_ij g_j and D columns dropped; D rows: char_diag
+ * on the diagonal, f_i = g_i * char_diag.                                      */
+int geo_apply_dirichlet_bcs(geo_ctx* ctx, const geo_csr* K, const double* f, const geo_dofs* dofs,
+                            geo_csr** K_bc, double* f_bc);
+/* Assembler::assemble_elasticity_stiffness_parallel, assembly.rs:389-437
+ * (GEO_ERR_INVALID_ARG unless 3 DOFs per node, as the reference's assert at :394). */
+int geo_assemble_elasticity_stiffness(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs,
+                                      const double* E_e, double E, double nu, geo_csr** K);
+/* Assembler::assemble_gravity_load, assembly.rs:906-937 */
+int geo_assemble_gravity_load(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs,
+                              double density, const double gravity[3], double* f);
+
+/* sprs CsMat<f64> stand-in (device resident). */
+int geo_csr_create(geo_ctx* ctx, int64_t n_rows, int64_t n_cols, int64_t nnz, const int64_t* indptr,
+                   const int32_t* indices, const double* data, geo_csr** out);
+int geo_csr_info(const geo_csr* A, int64_t* n_rows, int64_t* n_cols, int64_t* nnz);
+int geo_csr_copy(const geo_csr* A, int64_t* indptr, int32_t* indices, double* data);
+int geo_csr_device_ptrs(const geo_csr* A, const int64_t** indptr, const int32_t** indices,
+                        const double** data);
+/* impl LinearOperator for CsMat<f64>, linalg/solver.rs:61-73: y = A x */
+int geo_csr_apply(geo_ctx* ctx, const geo_csr* A, const double* x, double* y);
+int geo_csr_destroy(geo_csr* A);
+
+/* ------------------------------------------------------------------ K4: FP64 Jacobi-PCG */
+void geo_cg_opts_default(geo_cg_opts* opts);
+/* ConjugateGradient::solve, iterative.rs:123-131 -> solve_with_operator_internal
+ * :46-119 with JacobiPreconditioner::new, preconditioner.rs:37-51. x0 = 0; stops when
+ * ||r|| < tol ||b|| or ||r|| < abs_tol; returns zeros when ||b|| < 1e-25.
+ * One persistent kernel runs the whole solve.                                  */
+int geo_cg_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_opts* opts,
+                 double* x, geo_solver_stats* stats);
+
+/* ------------------------------------------------------------------ K5/K6: matrix-free */
+/* Matrix-free Dirichlet-eliminated operator K_bc of the thermal problem (the
+ * operator apply_dirichlet_bcs(assemble_thermal_stiffness_parallel(..)) builds,
+ * assembly.rs:69-117 + :168-230) or of 3-DOF elasticity (assembly.rs:389-437).
+ * Replaces the Solver::solve_with_operator seam, linalg/solver.rs:112-120.     */
+int geo_thermal_operator_create(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs,
+                                const double* k_e, double k, geo_op** out);
+int geo_elasticity_operator_create(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs,
+                                   const double* E_e, double E, double nu, geo_op** out);
+/* Replace the per-element coefficients (k_e or E_e; NULL -> uniform scalar). */
+int geo_op_set_coefficients(geo_op* op, const double* coef_e, double coef);
+int geo_op_info(const geo_op* op, int64_t* n_dofs, int64_t* n_elem, double* char_diag);
+/* y = K_bc x (LinearOperator::apply, linalg/solver.rs:41-58); precision FP64 or MIXED
+ * (MIXED applies the FP32 operator to the FP32-rounded x). */
+int geo_op_apply(geo_op* op, const double* x, double* y, int32_t precision);
+/* The vector half of apply_dirichlet_bcs (assembly.rs:195-218), matrix-free. */
+int geo_op_lift_rhs(geo_op* op, const double* f, double* f_bc);
+/* diag(K_bc), the Jacobi diagonal (preconditioner.rs:37-51). */
+int geo_op_diagonal(geo_op* op, double* diag);
+/* Jacobi-PCG on K_bc in one persistent kernel (matvec, Jacobi scaling, axpys and
+ * grid-reduced dot products). FP64: the reference's stopping rule on the recursive
+ * residual. MIXED: FP32 inner PCG with FP32 accumulation; the FP64 residual
+ * b - A x and the FP64 solution update are refreshed on device whenever the FP32
+ * residual fell by opts.reliable_delta; convergence is decided on the FP64 residual. */
+int geo_cg_solve_matfree(geo_op* op, const double* b, const geo_cg_opts* opts, double* x,
+                         geo_solver_stats* stats);
+
+/* ------------------------------------------------------------------ K7: adjoint (vjp) */
+/* Per-element g_e = -lambda_e^T K_e u_e, lambda zeroed on Dirichlet DOFs. For the
+ * thermal operator this is dJ/d(ln k_e); for elasticity dJ/d(ln E_e).        */
+int geo_op_element_gradient(geo_op* op, const double* u, const double* lambda, double* grad_e);
+/* forward: u = K_bc^{-1} lift(f)  (apply_dirichlet_bcs + ConjugateGradient::solve) */
+int geo_forward(geo_op* op, const double* f, const geo_cg_opts* opts, double* u,
+                geo_solver_stats* stats);
+/* backward (vector-Jacobian product): given dJ/du, solve K_bc lambda = dJ/du (free
+ * rows) and return dJ/d(ln coef_e). u may be NULL: the forward solution is then
+ * recomputed from f (recompute instead of store).                             */
+int geo_vjp(geo_op* op, const double* f, const double* u, const double* dJ_du,
+            const geo_cg_opts* opts, double* dJ_dlncoef, geo_solver_stats* stats);
+int geo_op_destroy(geo_op* op);
+
+/* ------------------------------------------------------------------ failure detection */
+/* Launches a persistent kernel whose block 0 skips one grid barrier on purpose so
+ * that every other block's bounded wait runs out after timeout_seconds; returns
+ * GEO_ERR_TIMEOUT when the device-side timeout fired and the context stays usable. */
+int geo_debug_barrier_timeout(geo_ctx* ctx, double timeout_seconds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GEO_FEM_H */

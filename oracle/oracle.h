@@ -1,0 +1,107 @@
+/*
+ * CPU oracle for the GeoSimulator Tet10 hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain C++ restatement of the reference's arithmetic (msahamed/geo_simulator,
+ * Rust), used by tests/, __graft_entry__.smoke() and the cpu_baseline leg of
+ * bench.py as the checker. The product library (geo_simulator_b200/libgeofem.so)
+ * never links, loads or calls it.
+ *
+ * Parity pinning: the reference cannot be compiled here (no Rust toolchain), so
+ * this restatement is pinned against every known-answer test the reference holds
+ * for the path (basis/quadrature/element/CG/Jacobi/LU/mesh-generator unit tests,
+ * the curved-element test, the shape-function benchmarks and the analytic
+ * thermal / patch-test solutions); see tests/test_oracle_pins.py.
+ *
+ * Every function names the reference lines it follows.  All arrays are
+ * row-major; node coordinates are AoS [n][3]; connectivity is [E][10] int64.
+ */
+#ifndef GEOFEM_ORACLE_H
+#define GEOFEM_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_mesh orc_mesh;
+typedef struct orc_csr orc_csr;
+
+typedef struct {
+    int64_t iterations;
+    double residual_norm;
+    double relative_residual;
+    int32_t converged;
+    double solve_time;
+} orc_stats;
+
+/* ---- mesh generator: mesh_generator_improved.rs:19-169 (HashMap edge cache) ---- */
+orc_mesh* orc_generate_cube(int64_t nx, int64_t ny, int64_t nz, double lx, double ly, double lz);
+int64_t orc_mesh_num_nodes(const orc_mesh* m);
+int64_t orc_mesh_num_elements(const orc_mesh* m);
+void orc_mesh_copy(const orc_mesh* m, double* xyz, int64_t* conn);
+void orc_mesh_free(orc_mesh* m);
+
+/* ---- basis / quadrature: basis.rs:56-276, 352-361; quadrature.rs:13-103 ---- */
+void orc_shape_functions(const double L[4], double N[10]);
+void orc_shape_derivatives_barycentric(const double L[4], double dN[40]);
+void orc_jacobian(const double L[4], const double nodes[30], double J[9]);
+double orc_det3(const double J[9]);
+int orc_shape_derivatives_cartesian(const double L[4], const double nodes[30], double dNdx[30]);
+double orc_element_volume(const double nodes[30]);
+/* rule: 1, 4, 5 or 11 points; returns number of points written */
+int orc_quadrature(int rule, double pts[44], double w[11]);
+
+/* ---- element matrices: element.rs:23-140 and the mechanics element files ---- */
+int orc_thermal_stiffness(const double nodes[30], double k, double Ke[100]);
+int orc_thermal_mass(const double nodes[30], double rho, double cp, double Me[100]);
+int orc_thermal_load(const double nodes[30], double Q, double fe[10]);
+void orc_constitutive_matrix(double E, double nu, double D[36]);
+void orc_b_matrix(const double dNdx[30], double B[180]);
+int orc_elasticity_stiffness(const double nodes[30], double E, double nu, double Ke[900]);
+int orc_gravity_load(const double nodes[30], double rho, const double g[3], double fe[30]);
+
+/* ---- assembly: assembly.rs:22-230, 389-437, 906-937 ---- */
+/* k_e: per-element conductivity (NULL -> uniform k); parallel != 0 uses the
+ * OpenMP element loop + serial triplet merge of the _parallel variant.        */
+orc_csr* orc_assemble_thermal_stiffness(int64_t n_nodes, const double* xyz, int64_t n_elem,
+                                        const int64_t* conn, const double* k_e, double k,
+                                        int parallel);
+void orc_assemble_thermal_load(int64_t n_nodes, const double* xyz, int64_t n_elem,
+                               const int64_t* conn, double Q, double* f);
+orc_csr* orc_assemble_elasticity_stiffness(int64_t n_nodes, const double* xyz, int64_t n_elem,
+                                           const int64_t* conn, const double* E_e, double E,
+                                           double nu, int parallel);
+void orc_assemble_gravity_load(int64_t n_nodes, const double* xyz, int64_t n_elem,
+                               const int64_t* conn, double rho, const double g[3], double* f);
+/* dirichlet_mask[n] (0/1) and values[n] per DOF (dof.rs:113-140)            */
+orc_csr* orc_apply_dirichlet_bcs(const orc_csr* K, const double* f, const uint8_t* dirichlet_mask,
+                                 const double* dirichlet_values, double* f_out);
+double orc_char_diag(const orc_csr* K);
+
+/* ---- sparse matrices (sprs TriMat::to_csr semantics) ---- */
+orc_csr* orc_csr_from_triplets(int64_t n_rows, int64_t n_cols, int64_t n_trip, const int64_t* rows,
+                               const int64_t* cols, const double* vals);
+int64_t orc_csr_rows(const orc_csr* A);
+int64_t orc_csr_nnz(const orc_csr* A);
+void orc_csr_copy(const orc_csr* A, int64_t* indptr, int64_t* indices, double* data);
+void orc_csr_apply(const orc_csr* A, const double* x, double* y);
+void orc_csr_free(orc_csr* A);
+
+/* ---- solvers: iterative.rs:46-131, preconditioner.rs:37-72, direct.rs:28-73 ---- */
+void orc_cg_solve(const orc_csr* A, const double* b, int64_t max_iterations, double tolerance,
+                  double abs_tolerance, int use_preconditioner, double* x, orc_stats* stats);
+int orc_lu_solve(const orc_csr* A, const double* b, double* x, orc_stats* stats);
+
+/* ---- adjoint checker (no reference counterpart): per-element
+ *      g_e = -lambda_e^T K_e u_e, with lambda already zero on Dirichlet DOFs -- */
+void orc_thermal_element_gradient(int64_t n_nodes, const double* xyz, int64_t n_elem,
+                                  const int64_t* conn, const double* k_e, const double* u,
+                                  const double* lam, double* g);
+void orc_elasticity_element_gradient(int64_t n_nodes, const double* xyz, int64_t n_elem,
+                                     const int64_t* conn, const double* E_e, double nu,
+                                     const double* u, const double* lam, double* g);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
