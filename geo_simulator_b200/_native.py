@@ -50,7 +50,7 @@ class SolverStatsC(C.Structure):
     _fields_ = [("iterations", C.c_int64), ("residual_norm", C.c_double),
                 ("relative_residual", C.c_double), ("converged", C.c_int32), ("solve_time", C.c_double),
                 ("status", C.c_int32), ("fp64_residual_updates", C.c_int64), ("b_norm", C.c_double),
-                ("kernel_time", C.c_double)]
+                ("kernel_time", C.c_double), ("kernel_launches", C.c_int64)]
 
 
 _P = C.c_void_p
@@ -65,6 +65,7 @@ _SIGS = {
     "geo_ctx_create": [C.c_int, _PP],
     "geo_ctx_destroy": [_P],
     "geo_sm_count": [_P, C.POINTER(C.c_int)],
+    "geo_ctx_stream": [_P, _PP],
     "geo_generate_cube_size": [_I64, _I64, _I64, C.POINTER(_I64), C.POINTER(_I64)],
     "geo_generate_cube": [_I64, _I64, _I64, _D, _D, _D, _DP, _DP],
     "geo_mesh_create": [_P, _I64, _DP, _I64, _DP, _PP],

@@ -131,6 +131,12 @@ int geo_sm_count(const geo_ctx* ctx, int* sm_count) {
     return GEO_OK;
 }
 
+int geo_ctx_stream(const geo_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return GEO_ERR_INVALID_ARG;
+    *stream = (void*)ctx->stream;
+    return GEO_OK;
+}
+
 int geo_mesh_create(geo_ctx* ctx, int64_t n_nodes, const double* xyz, int64_t n_elem,
                     const int32_t* conn, geo_mesh** out) {
     GEO_API_BEGIN(ctx)
@@ -143,11 +149,6 @@ int geo_mesh_create(geo_ctx* ctx, int64_t n_nodes, const double* xyz, int64_t n_
     m->n_nodes = n_nodes;
     m->n_elem = n_elem;
     cudaStream_t s = ctx->stream;
-    // keep host copies for host-side operator set-up
-    m->h_xyz.resize(3 * n_nodes);
-    m->h_conn.resize(10 * n_elem);
-    GEO_CUDA(cudaMemcpyAsync(m->h_xyz.data(), xyz, 3 * n_nodes * sizeof(double), cudaMemcpyDefault, s));
-    GEO_CUDA(cudaMemcpyAsync(m->h_conn.data(), conn, 10 * n_elem * sizeof(int32_t), cudaMemcpyDefault, s));
     DevBuf<double> txyz;
     DevBuf<int32_t> tconn;
     const double* dxyz = stage_in(xyz, 3 * n_nodes, txyz, s);

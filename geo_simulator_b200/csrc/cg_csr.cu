@@ -212,6 +212,7 @@ int geo_cg_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_o
     }
     const int status = r.converged ? GEO_OK : (r.breakdown ? GEO_ERR_BREAKDOWN : GEO_NOT_CONVERGED);
     fill_stats(stats, r, ms * 1e-3, status);
+    if (stats) stats->kernel_launches = 1;
     if (status != GEO_OK) {
         record_error(ctx, status, r.breakdown ? "CG breakdown: |p^T A p| < 1e-30" : "CG did not converge");
         return status;

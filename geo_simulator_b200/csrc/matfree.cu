@@ -14,344 +14,12 @@
 #include <cmath>
 #include <type_traits>
 
-#include "matfree.cuh"
-#include "patches.h"
+#include "mf_kernels.cuh"
 #include "pcg_common.cuh"
 
 struct geo_op;
 
 namespace geo {
-
-constexpr int kMfBS = 128;
-
-enum ApplyMode : int { MODE_FREE = 0, MODE_LIFT = 1 };
-
-struct PatchView {
-    int64_t E, N;
-    int n_patches, ucap, dpn;
-    const int32_t* pe;
-    const int32_t* po;
-    const int32_t* pf;
-    const int32_t* foreign;
-    const uint16_t* lconn;
-    const uint8_t* flags;
-};
-
-// One patch-ordered pass y (+)= K x over all patches handled by this block
-// (patch = blockIdx.x, += gridDim.x). D-row outputs are left untouched; in
-// MODE_FREE Dirichlet inputs are read as zero, in MODE_LIFT free inputs are.
-// Returns this thread's share of x^T y over the elements (masked x).
-template <class K, class T>
-__device__ double element_phase(const PatchView& pv, const T* __restrict__ qd, T cl, T cm, const T* __restrict__ x,
-                                T* __restrict__ y, void* smem_raw, int mode) {
-    constexpr int DPN = K::DPN;
-    T* sx = reinterpret_cast<T*>(smem_raw);
-    T* sy = sx + pv.ucap * DPN;
-    double dot = 0.0;
-    for (int patch = blockIdx.x; patch < pv.n_patches; patch += gridDim.x) {
-        const int e0 = pv.pe[patch], e1 = pv.pe[patch + 1];
-        const int o0 = pv.po[patch], nown = pv.po[patch + 1] - o0;
-        const int f0 = pv.pf[patch], nloc = nown + pv.pf[patch + 1] - f0;
-        for (int u = threadIdx.x; u < nloc; u += blockDim.x) {
-            const int node = u < nown ? o0 + u : pv.foreign[f0 + u - nown];
-            const uint8_t fl = pv.flags[node];
-#pragma unroll
-            for (int c = 0; c < DPN; ++c) {
-                T v = x[(int64_t)node * DPN + c];
-                const bool dir = (fl >> c) & 1;
-                if (mode == MODE_FREE ? dir : !dir) v = T(0);
-                sx[u * DPN + c] = v;
-                sy[u * DPN + c] = T(0);
-            }
-        }
-        __syncthreads();
-        for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-            int li[10];
-#pragma unroll
-            for (int l = 0; l < 10; ++l) li[l] = pv.lconn[(int64_t)l * pv.E + e];
-            T xe[10 * DPN], ye[10 * DPN];
-#pragma unroll
-            for (int l = 0; l < 10; ++l)
-#pragma unroll
-                for (int c = 0; c < DPN; ++c) xe[l * DPN + c] = sx[li[l] * DPN + c];
-            K::apply(qd, pv.E, e, cl, cm, xe, ye);
-            T d = T(0);
-#pragma unroll
-            for (int k = 0; k < 10 * DPN; ++k) d += xe[k] * ye[k];
-            dot += (double)d;
-#pragma unroll
-            for (int l = 0; l < 10; ++l)
-#pragma unroll
-                for (int c = 0; c < DPN; ++c) atomicAdd(&sy[li[l] * DPN + c], ye[l * DPN + c]);
-        }
-        __syncthreads();
-        for (int u = threadIdx.x; u < nloc; u += blockDim.x) {
-            const int node = u < nown ? o0 + u : pv.foreign[f0 + u - nown];
-            const uint8_t fl = pv.flags[node];
-            const bool plain = u < nown && !(fl & kFlagShared);
-#pragma unroll
-            for (int c = 0; c < DPN; ++c) {
-                if ((fl >> c) & 1) continue;
-                const T v = sy[u * DPN + c];
-                T* dst = y + (int64_t)node * DPN + c;
-                if (plain) *dst = v;
-                else atomicAdd(dst, v);
-            }
-        }
-        __syncthreads();
-    }
-    return dot;
-}
-
-struct MfArgs {
-    PatchView pv;
-    const double* qd64;
-    const float* qd32;
-    double cl, cm, cd;
-    int64_t ndof;
-    const double* b;          // right-hand side, patch numbering
-    double* x64;              // solution (FP64)
-    double *r64, *p64, *q64;  // FP64 mode vectors
-    const double* dinv64;
-    float *xs, *r32, *p32, *q32;  // MIXED inner vectors
-    const float* dinv32;
-    double* w64;  // MIXED: K x64, then b - K x64
-    double *part_a, *part_b, *part_c;
-    GridSync* gs;
-    PcgResult* res;
-    unsigned long long timeout_ns;
-    long long max_it;
-    double tol, abs_tol, delta;
-};
-
-#define MF_BARRIER()                                   \
-    do {                                               \
-        if (!grid_barrier(a.gs, nb, a.timeout_ns)) return; \
-    } while (0)
-
-// Persistent Jacobi-PCG over the matrix-free operator.
-//  FP64: the reference loop (iterative.rs:46-119) with its stopping rule on the
-//        recursive residual.
-//  MIXED: the same loop on FP32 vectors with the FP32 operator; x accumulates
-//        in FP32 (xs) and is flushed into the FP64 solution whenever the FP32
-//        residual fell by `delta` since the last refresh, at which point the
-//        true residual b - K x is recomputed in FP64, the FP32 residual is
-//        replaced by it (rescaled to unit norm) and the search direction is kept.
-//        Convergence is decided on that FP64 residual.
-template <class K64, class K32, bool MIXED>
-__global__ void __launch_bounds__(kMfBS) k_mf_pcg(MfArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    constexpr int DPN = K64::DPN;
-    using T = typename std::conditional<MIXED, float, double>::type;
-    using KT = typename std::conditional<MIXED, K32, K64>::type;
-    const unsigned nb = gridDim.x;
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
-    const int64_t n = a.ndof;
-    const uint8_t* flags = a.pv.flags;
-    const double cd = a.cd;
-    T* xv = MIXED ? (T*)a.xs : (T*)a.x64;
-    T* rv = MIXED ? (T*)a.r32 : (T*)a.r64;
-    T* pv = MIXED ? (T*)a.p32 : (T*)a.p64;
-    T* qv = MIXED ? (T*)a.q32 : (T*)a.q64;
-    const T* dv = MIXED ? (const T*)a.dinv32 : (const T*)a.dinv64;
-    const T* qd = MIXED ? (const T*)a.qd32 : (const T*)a.qd64;
-
-    double bnorm, rz, s_scale = 1.0;
-    double pdd = 0.0;  // this block's sum of p_i^2 over Dirichlet rows
-    {
-        double v[2] = {0.0, 0.0};
-        for (int64_t i = tid; i < n; i += nth) {
-            const double bi = a.b[i];
-            v[0] += bi * bi;
-            if (!MIXED) {
-                const double zi = bi * a.dinv64[i];
-                a.x64[i] = 0.0;
-                a.r64[i] = bi;
-                a.p64[i] = zi;
-                v[1] += bi * zi;
-                if ((flags[i / DPN] >> (i % DPN)) & 1) pdd += zi * zi;
-            } else {
-                a.x64[i] = 0.0;
-                a.xs[i] = 0.0f;
-            }
-        }
-        store_partial<2>(a.part_b, v);
-    }
-    MF_BARRIER();
-    {
-        double t[2];
-        grid_total<2>(a.part_b, nb, t);
-        bnorm = sqrt(t[0]);
-        rz = t[1];
-    }
-    if (bnorm < 1e-25) {
-        if (tid == 0) *a.res = PcgResult{0, 0.0, bnorm, 1, 0, 0};
-        return;
-    }
-    if (MIXED) {
-        s_scale = bnorm;
-        double v[1] = {0.0};
-        const double inv = 1.0 / s_scale;
-        for (int64_t i = tid; i < n; i += nth) {
-            const float ri = (float)(a.b[i] * inv);
-            const float zi = ri * a.dinv32[i];
-            a.r32[i] = ri;
-            a.p32[i] = zi;
-            v[0] += (double)(ri * zi);
-            if ((flags[i / DPN] >> (i % DPN)) & 1) pdd += (double)(zi * zi);
-        }
-        store_partial<1>(a.part_c, v);
-        MF_BARRIER();
-        double t[1];
-        grid_total<1>(a.part_c, nb, t);
-        rz = t[0];
-    }
-    long long it = 0, nupd = 0;
-    int converged = 0, breakdown = 0;
-    double final_res = bnorm, rmax = 1.0;
-    while (it < a.max_it) {
-        // ---- q = K_bc p (free rows by elements; Dirichlet rows folded in below)
-        {
-            double v[1];
-            v[0] = element_phase<KT, T>(a.pv, qd, (T)a.cl, (T)a.cm, pv, qv, smem, MODE_FREE);
-            v[0] += cd * pdd;
-            store_partial<1>(a.part_a, v);
-        }
-        MF_BARRIER();
-        double pq[1];
-        grid_total<1>(a.part_a, nb, pq);
-        if (fabs(pq[0]) < 1e-30) {
-            breakdown = 1;
-            break;
-        }
-        const T alpha = (T)(rz / pq[0]);
-        {
-            T acc_rr = T(0), acc_rz = T(0);
-            for (int64_t i = tid; i < n; i += nth) {
-                const uint8_t fl = flags[i / DPN];
-                const bool dir = (fl >> (i % DPN)) & 1;
-                const T pi = pv[i];
-                T qi;
-                if (dir) {
-                    qi = (T)cd * pi;
-                } else {
-                    qi = qv[i];
-                    if (fl & kFlagShared) qv[i] = T(0);
-                }
-                xv[i] += alpha * pi;
-                const T ri = rv[i] - alpha * qi;
-                rv[i] = ri;
-                acc_rr += ri * ri;
-                acc_rz += ri * (ri * dv[i]);
-            }
-            double v[2] = {(double)acc_rr, (double)acc_rz};
-            store_partial<2>(a.part_b, v);
-        }
-        MF_BARRIER();
-        double t2[2];
-        grid_total<2>(a.part_b, nb, t2);
-        double rz_new = t2[1];
-        const double rn = sqrt(t2[0]);
-        if (!MIXED) {
-            final_res = rn;
-            if (rn < a.tol * bnorm || rn < a.abs_tol) {
-                converged = 1;
-                break;
-            }
-        } else {
-            rmax = fmax(rmax, rn);
-            const double est = rn * s_scale;
-            if (est < a.tol * bnorm || est < a.abs_tol || rn < a.delta * rmax) {
-                // ---- refresh: x64 += s xs, xs = 0
-                for (int64_t i = tid; i < n; i += nth) {
-                    a.x64[i] += s_scale * (double)a.xs[i];
-                    a.xs[i] = 0.0f;
-                }
-                MF_BARRIER();
-                // ---- w = K_bc x64 (FP64 operator)
-                element_phase<K64, double>(a.pv, a.qd64, a.cl, a.cm, a.x64, a.w64, smem, MODE_FREE);
-                MF_BARRIER();
-                // ---- w = b - K_bc x64 and its norm
-                {
-                    double v[1] = {0.0};
-                    for (int64_t i = tid; i < n; i += nth) {
-                        const bool dir = (flags[i / DPN] >> (i % DPN)) & 1;
-                        const double kx = dir ? cd * a.x64[i] : a.w64[i];
-                        const double ri = a.b[i] - kx;
-                        a.w64[i] = ri;
-                        v[0] += ri * ri;
-                    }
-                    store_partial<1>(a.part_c, v);
-                }
-                MF_BARRIER();
-                double t1[1];
-                grid_total<1>(a.part_c, nb, t1);
-                const double s_new = sqrt(t1[0]);
-                ++nupd;
-                final_res = s_new;
-                if (s_new < a.tol * bnorm || s_new < a.abs_tol) {
-                    converged = 1;
-                    break;
-                }
-                // ---- r32 = (b - K x64) / s_new, p32 rescaled, rz recomputed
-                {
-                    const double ratio = s_scale / s_new, inv = 1.0 / s_new;
-                    double v[1] = {0.0};
-                    for (int64_t i = tid; i < n; i += nth) {
-                        const uint8_t fl = flags[i / DPN];
-                        const double wi = a.w64[i];
-                        if (!((fl >> (i % DPN)) & 1) && (fl & kFlagShared)) a.w64[i] = 0.0;
-                        const float ri = (float)(wi * inv);
-                        a.r32[i] = ri;
-                        a.p32[i] = (float)((double)a.p32[i] * ratio);
-                        v[0] += (double)(ri * (ri * a.dinv32[i]));
-                    }
-                    store_partial<1>(a.part_a, v);
-                    MF_BARRIER();
-                    double t1b[1];
-                    grid_total<1>(a.part_a, nb, t1b);
-                    rz *= ratio * ratio;
-                    rz_new = t1b[0];
-                    s_scale = s_new;
-                    rmax = 1.0;
-                }
-            }
-        }
-        const T beta = (T)(rz_new / rz);
-        rz = rz_new;
-        pdd = 0.0;
-        for (int64_t i = tid; i < n; i += nth) {
-            const T pnew = rv[i] * dv[i] + beta * pv[i];
-            pv[i] = pnew;
-            if ((flags[i / DPN] >> (i % DPN)) & 1) pdd += (double)(pnew * pnew);
-        }
-        MF_BARRIER();
-        ++it;
-    }
-    if (MIXED && !converged) {
-        for (int64_t i = tid; i < n; i += nth) {
-            a.x64[i] += s_scale * (double)a.xs[i];
-            a.xs[i] = 0.0f;
-        }
-    }
-    if (tid == 0) *a.res = PcgResult{it, final_res, bnorm, converged, breakdown, nupd};
-}
-
-// ------------------------------------------------------------------ stand-alone kernels
-template <class K, class T>
-__global__ void __launch_bounds__(kMfBS) k_mf_apply(PatchView pv, const T* qd, T cl, T cm, const T* x, T* y,
-                                                     int mode) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    element_phase<K, T>(pv, qd, cl, cm, x, y, smem, mode);
-}
-
-// y_D = cd x_D (MODE_FREE) for the Dirichlet rows after an element pass
-template <class T>
-__global__ void k_dir_rows(const uint8_t* flags, int dpn, int64_t n, double cd, const T* x, T* y) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        if ((flags[i / dpn] >> (i % dpn)) & 1) y[i] = (T)(cd * (double)x[i]);
-}
 
 // f_bc: free rows f - (K_{F,D} g), Dirichlet rows g cd
 __global__ void k_lift_finish(const uint8_t* flags, int dpn, int64_t n, double cd, const double* f,
@@ -387,6 +55,20 @@ __global__ void k_to_orig(const int32_t* nperm, int dpn, int64_t N, const Tin* i
 }
 
 // ------------------------------------------------------------------ set-up kernels
+// node flags (Dirichlet bits, shared bit) and Dirichlet values in patch numbering
+__global__ void k_node_flags(const int32_t* nperm, const uint8_t* shared, const uint8_t* mask, const double* vals,
+                             int dpn, int64_t N, uint8_t* flags, double* g_new) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = nperm[i];
+        uint8_t f = shared[i] ? kFlagShared : 0;
+        for (int c = 0; c < dpn; ++c) {
+            if (mask[o * dpn + c]) f |= (uint8_t)(kFlagDir0 << c);
+            g_new[i * dpn + c] = vals[o * dpn + c];
+        }
+        flags[i] = f;
+    }
+}
+
 __device__ __forceinline__ void load_elem(const double* __restrict__ xyz, const int32_t* __restrict__ conn,
                                           int64_t N, int64_t E, int64_t e, double (&X)[10][3]) {
 #pragma unroll
@@ -458,8 +140,9 @@ __global__ void k_qdata(int phys, const double* xyz, const int32_t* conn, const 
             G[4] = s * (A[1][0] * A[2][0] + A[1][1] * A[2][1] + A[1][2] * A[2][2]);
             G[5] = s * (A[2][0] * A[2][0] + A[2][1] * A[2][1] + A[2][2] * A[2][2]);
             for (int j = 0; j < 6; ++j) {
-                qd64[(6 * q + j) * E + ne] = G[j];
-                qd32[(6 * q + j) * E + ne] = (float)G[j];
+                const int64_t at = ((ne / kPatchElems) * (6 * NQ) + 6 * q + j) * kPatchElems + ne % kPatchElems;
+                qd64[at] = G[j];
+                qd32[at] = (float)G[j];
             }
         } else {
             double v[10];
@@ -467,8 +150,9 @@ __global__ void k_qdata(int phys, const double* xyz, const int32_t* conn, const 
                 for (int c = 0; c < 3; ++c) v[3 * r + c] = A[r][c] / d;
             v[9] = kQw * fabs(d) * k;
             for (int j = 0; j < 10; ++j) {
-                qd64[(10 * q + j) * E + ne] = v[j];
-                qd32[(10 * q + j) * E + ne] = (float)v[j];
+                const int64_t at = ((ne / kPatchElems) * (10 * NQ) + 10 * q + j) * kPatchElems + ne % kPatchElems;
+                qd64[at] = v[j];
+                qd32[at] = (float)v[j];
             }
         }
     }
@@ -617,10 +301,10 @@ struct geo_op {
     const geo_mesh* mesh = nullptr;
     int phys = 0, dpn = 1, nq = 1;
     int64_t N = 0, E = 0, ndof = 0;
-    int n_patches = 0, ucap = 0;
+    int n_patches = 0, max_local = 0;
     double nu = 0, cl = 0, cm = 0, cd = 1.0, coef_scalar = 1.0;
     geo::DevBuf<int32_t> eperm, nperm, pe, po, pf, foreign;
-    geo::DevBuf<uint16_t> lconn;
+    geo::DevBuf<uint32_t> lc;
     geo::DevBuf<uint8_t> flags;
     geo::DevBuf<uint8_t> mask_orig;  // Dirichlet mask, original DOF numbering
     geo::DevBuf<double> coef, qd64, g_new, diag_new, dinv64, ediag, diag_orig;
@@ -628,12 +312,27 @@ struct geo_op {
     // solver workspace
     geo::DevBuf<double> w64;
     geo::DevBuf<float> w32;
-    geo::PcgScratch sc;
-    int pcg_blocks[2][2] = {{0, 0}, {0, 0}};
+    geo::DevBuf<double> bvec, xvec;  // right-hand side and solution (patch numbering)
+    geo::DevBuf<geo::PcgState> state;
+    geo::DevBuf<double> part;
+    geo::PcgState* h_state = nullptr;  // pinned mirror
+    int patch_grid[2] = {0, 0};        // resident patch-kernel blocks (FP64, FP32)
+    int nbuf[2] = {2, 2};              // element-data buffers of the patch kernel (FP64, FP32)
+    int node_grid = 0;
+    // CUDA graphs of PCG iteration chunks, keyed by precision
+    cudaGraphExec_t chunk[2] = {nullptr, nullptr};
+    const void* chunk_key[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    ~geo_op() {
+        for (auto& g : chunk)
+            if (g) cudaGraphExecDestroy(g);
+        if (h_state) cudaFreeHost(h_state);
+    }
 };
 
 namespace geo {
 namespace {
+
+constexpr int kChunk = 16;  // PCG iterations per graph launch
 
 inline unsigned nblk(int64_t n, int bs = 256) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, bs), 148 * 64));
@@ -644,18 +343,25 @@ PatchView view(const geo_op* op) {
     v.E = op->E;
     v.N = op->N;
     v.n_patches = op->n_patches;
-    v.ucap = op->ucap;
+    v.max_local = op->max_local;
     v.dpn = op->dpn;
     v.pe = op->pe.p;
     v.po = op->po.p;
     v.pf = op->pf.p;
     v.foreign = op->foreign.p;
-    v.lconn = op->lconn.p;
+    v.lc = op->lc.p;
     v.flags = op->flags.p;
     return v;
 }
 
-size_t smem_bytes(const geo_op* op, size_t elt) { return (size_t)2 * op->ucap * op->dpn * elt; }
+// dynamic shared memory of the patch kernel: barriers, element-data buffers, node tables
+template <class K, class T>
+size_t smem_bytes(const geo_op* op, int nbuf) {
+    const size_t tables = (size_t)2 * op->max_local * K::DPN * sizeof(T) + (size_t)op->max_local * 5 + 16;
+    return (nbuf == 2 ? patch_smem_fixed<K, T, 2>() : patch_smem_fixed<K, T, 1>()) + tables;
+}
+
+constexpr size_t kSmemLimit = 227 * 1024;
 
 template <class F>
 void with_kernels(const geo_op* op, F&& f) {
@@ -669,9 +375,40 @@ void with_kernels(const geo_op* op, F&& f) {
     }
 }
 
+template <class K, class T, int NBUF>
+int setup_patch_nbuf(geo_ctx* ctx, size_t bytes) {
+    GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_FREE, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bytes));
+    GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_LIFT, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bytes));
+    GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_PCG, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bytes));
+    int per_sm = 0;
+    GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_patch<K, T, MODE_PCG, NBUF>, kPatchBS, bytes));
+    if (per_sm < 1) fail(GEO_ERR_UNSUPPORTED, "patch kernel does not fit on an SM");
+    return per_sm * ctx->sm_count;
+}
+
+// Picks double buffering when it fits in shared memory; returns the resident grid.
 template <class K, class T>
-void set_smem_attr(size_t bytes) {
-    GEO_CUDA(cudaFuncSetAttribute(k_mf_apply<K, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+int setup_patch_kernels(geo_op* op, int slot) {
+    if (smem_bytes<K, T>(op, 2) <= kSmemLimit) {
+        op->nbuf[slot] = 2;
+        return setup_patch_nbuf<K, T, 2>(op->ctx, smem_bytes<K, T>(op, 2));
+    }
+    if (smem_bytes<K, T>(op, 1) > kSmemLimit)
+        fail(GEO_ERR_UNSUPPORTED, "patch tables exceed shared memory (too many nodes per patch)");
+    op->nbuf[slot] = 1;
+    return setup_patch_nbuf<K, T, 1>(op->ctx, smem_bytes<K, T>(op, 1));
+}
+
+template <class K, class T, int MODE>
+void launch_patch(const geo_op* op, int slot, cudaStream_t s, const T* qd, const PatchArgs<T>& pa) {
+    const unsigned g = (unsigned)std::min(op->patch_grid[slot], op->n_patches);
+    if (op->nbuf[slot] == 2)
+        k_patch<K, T, MODE, 2><<<g, kPatchBS, smem_bytes<K, T>(op, 2), s>>>(view(op), qd, (T)op->cl, (T)op->cm, pa);
+    else
+        k_patch<K, T, MODE, 1><<<g, kPatchBS, smem_bytes<K, T>(op, 1), s>>>(view(op), qd, (T)op->cl, (T)op->cm, pa);
 }
 
 // Recomputes qdata, diagonal, char_diag and the Jacobi inverse from op->coef.
@@ -681,8 +418,10 @@ void refresh_coefficients(geo_op* op) {
     const geo_mesh* m = op->mesh;
     reset_dev_err(ctx);
     const int nqd = (op->phys == 0 ? 6 : 10) * op->nq;
-    op->qd64.ensure((size_t)nqd * op->E);
-    op->qd32.ensure((size_t)nqd * op->E);
+    op->qd64.ensure((size_t)nqd * op->n_patches * kPatchElems);
+    op->qd32.ensure((size_t)nqd * op->n_patches * kPatchElems);
+    GEO_CUDA(cudaMemsetAsync(op->qd64.p, 0, op->qd64.bytes(), s));
+    GEO_CUDA(cudaMemsetAsync(op->qd32.p, 0, op->qd32.bytes(), s));
     if (op->nq == 1)
         k_qdata<1><<<(unsigned)cdiv(op->E, 128), 128, 0, s>>>(op->phys, m->xyz.p, m->conn.p, op->eperm.p, op->N, op->E,
                                                     op->coef.p, op->qd64.p, op->qd32.p, ctx->dev_err.p);
@@ -753,41 +492,24 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
     cudaStream_t s = ctx->stream;
     ensure_inverse_map(const_cast<geo_mesh*>(mesh));
     PatchLayout L;
-    try {
-        build_patches(op->N, mesh->h_xyz.data(), op->E, mesh->h_conn.data(), L);
-    } catch (const std::exception& ex) {
-        fail(GEO_ERR_UNSUPPORTED, ex.what());
-    }
-    op->n_patches = (int)L.n_patches;
-    op->ucap = L.max_local;
-    // node flags in patch numbering: Dirichlet bit per component + shared bit
-    std::vector<uint8_t> fl(op->N, 0);
-    for (int64_t i = 0; i < op->N; ++i) {
-        const int64_t o = L.nperm[i];
-        uint8_t f = L.shared[i] ? kFlagShared : 0;
-        for (int c = 0; c < dpn; ++c)
-            if (dofs->h_mask[o * dpn + c]) f |= (uint8_t)(kFlagDir0 << c);
-        fl[i] = f;
-    }
-    std::vector<double> gnew(op->ndof);
-    for (int64_t i = 0; i < op->N; ++i)
-        for (int c = 0; c < dpn; ++c) gnew[i * dpn + c] = dofs->h_vals[(int64_t)L.nperm[i] * dpn + c];
-    auto up = [&](auto& buf, const auto& vec) {
-        buf.alloc(std::max<size_t>(vec.size(), 1));
-        if (!vec.empty())
-            GEO_CUDA(cudaMemcpyAsync(buf.p, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, s));
-    };
-    up(op->eperm, L.eperm);
-    up(op->nperm, L.nperm);
-    up(op->pe, L.patch_elem);
-    up(op->po, L.patch_own);
-    up(op->pf, L.patch_foreign);
-    up(op->foreign, L.foreign);
-    up(op->lconn, L.lconn);
-    up(op->flags, fl);
-    up(op->g_new, gnew);
-    up(op->mask_orig, dofs->h_mask);
-    sync(ctx, "operator upload");
+    build_patches(s, op->N, mesh->xyz.p, op->E, mesh->conn.p, L);
+    op->n_patches = L.n_patches;
+    op->max_local = L.max_local;
+    op->eperm = std::move(L.eperm);
+    op->nperm = std::move(L.nperm);
+    op->pe = std::move(L.patch_elem);
+    op->po = std::move(L.patch_own);
+    op->pf = std::move(L.patch_foreign);
+    op->foreign = std::move(L.foreign);
+    op->lc = std::move(L.lc);
+    op->mask_orig.alloc(op->ndof);
+    GEO_CUDA(cudaMemcpyAsync(op->mask_orig.p, dofs->mask.p, op->ndof, cudaMemcpyDeviceToDevice, s));
+    op->flags.alloc(op->N);
+    op->g_new.alloc(op->ndof);
+    k_node_flags<<<nblk(op->N), 256, 0, s>>>(op->nperm.p, L.shared.p, dofs->mask.p, dofs->vals.p, dpn, op->N,
+                                             op->flags.p, op->g_new.p);
+    check_launch(ctx, "k_node_flags");
+    sync(ctx, "operator layout");
     // affine (straight-sided) elements use one metric per element
     DevBuf<int> aff(1);
     GEO_CUDA(cudaMemsetAsync(aff.p, 0, sizeof(int), s));
@@ -802,15 +524,16 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
     with_kernels(op.get(), [&](auto k64, auto k32) {
         using K64 = decltype(k64);
         using K32 = decltype(k32);
-        set_smem_attr<K64, double>(smem_bytes(op.get(), 8));
-        set_smem_attr<K32, float>(smem_bytes(op.get(), 4));
-        GEO_CUDA(cudaFuncSetAttribute(k_mf_pcg<K64, K32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_bytes(op.get(), 8)));
-        GEO_CUDA(cudaFuncSetAttribute(k_mf_pcg<K64, K32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_bytes(op.get(), 8)));
-        op->pcg_blocks[0][0] = persistent_blocks(ctx, k_mf_pcg<K64, K32, false>, kMfBS, smem_bytes(op.get(), 8));
-        op->pcg_blocks[0][1] = persistent_blocks(ctx, k_mf_pcg<K64, K32, true>, kMfBS, smem_bytes(op.get(), 8));
+        op->patch_grid[0] = setup_patch_kernels<K64, double>(op.get(), 0);
+        op->patch_grid[1] = setup_patch_kernels<K32, float>(op.get(), 1);
     });
+    op->node_grid = ctx->sm_count * 8;
+    op->bvec.alloc(op->ndof);
+    op->xvec.alloc(op->ndof);
+    op->state.alloc(1);
+    op->part.alloc((size_t)2 * std::max({op->patch_grid[0], op->patch_grid[1], op->node_grid}));
+    GEO_CUDA(cudaMemset(op->state.p, 0, sizeof(PcgState)));
+    GEO_CUDA(cudaMallocHost(&op->h_state, sizeof(PcgState)));
     return op.release();
 }
 
@@ -820,18 +543,24 @@ void apply_new(geo_op* op, const T* x, T* y, int mode) {
     geo_ctx* ctx = op->ctx;
     cudaStream_t s = ctx->stream;
     GEO_CUDA(cudaMemsetAsync(y, 0, op->ndof * sizeof(T), s));
-    const PatchView pv = view(op);
+    constexpr bool dbl = std::is_same<T, double>::value;
+    reset_dev_err(ctx);
     with_kernels(op, [&](auto k64, auto k32) {
-        using K = typename std::conditional<std::is_same<T, double>::value, decltype(k64), decltype(k32)>::type;
-        const T* qd = std::is_same<T, double>::value ? (const T*)op->qd64.p : (const T*)op->qd32.p;
-        k_mf_apply<K, T><<<(unsigned)op->n_patches, kMfBS, smem_bytes(op, sizeof(T)), s>>>(
-            pv, qd, (T)op->cl, (T)op->cm, x, y, mode);
+        using K = typename std::conditional<dbl, decltype(k64), decltype(k32)>::type;
+        const T* qd = dbl ? (const T*)op->qd64.p : (const T*)op->qd32.p;
+        PatchArgs<T> pa{};
+        pa.x = x;
+        pa.y = y;
+        pa.err = ctx->dev_err.p;
+        if (mode == MODE_FREE) launch_patch<K, T, MODE_FREE>(op, dbl ? 0 : 1, s, qd, pa);
+        else launch_patch<K, T, MODE_LIFT>(op, dbl ? 0 : 1, s, qd, pa);
     });
-    check_launch(ctx, "k_mf_apply");
+    check_launch(ctx, "k_patch");
     if (mode == MODE_FREE) {
         k_dir_rows<T><<<nblk(op->ndof), 256, 0, s>>>(op->flags.p, op->dpn, op->ndof, op->cd, x, y);
         check_launch(ctx, "k_dir_rows");
     }
+    raise_dev_err(ctx, read_dev_err(ctx), "matrix-free apply");
 }
 
 void to_new(geo_op* op, const double* in_orig, double* out_new) {
@@ -857,78 +586,148 @@ void lift_new(geo_op* op, const double* f_orig_dev, double* fbc_new) {
     sync(op->ctx, "lift");
 }
 
-// Persistent PCG on K_bc; b_new / x_new in patch numbering (device).
-int solve_new(geo_op* op, const double* b_new, const geo_cg_opts& o, double* x_new, geo_solver_stats* st) {
+// Enqueues one PCG iteration (patch kernel in PCG mode + node update).
+template <class K, class T, bool MIXED>
+void enqueue_iteration(geo_op* op, cudaStream_t s, const PatchArgs<T>& pa, const NodeArgs<T>& na) {
+    constexpr bool dbl = std::is_same<T, double>::value;
+    const T* qd = dbl ? (const T*)op->qd64.p : (const T*)op->qd32.p;
+    launch_patch<K, T, MODE_PCG>(op, dbl ? 0 : 1, s, qd, pa);
+    k_pcg_update<T, K::DPN, MIXED><<<(unsigned)op->node_grid, kNodeBS, 0, s>>>(na);
+}
+
+// Jacobi-PCG on K_bc; b_new / x_new in patch numbering (device). Iterations run
+// in CUDA-graph chunks of kChunk (kernels turn into no-ops once the device state
+// says done or refresh); the host looks at the state between chunks and runs the
+// FP64 refresh of the mixed solver when it is requested.
+int solve_new(geo_op* op, const geo_cg_opts& o, geo_solver_stats* st) {
     geo_ctx* ctx = op->ctx;
+    const double* b_new = op->bvec.p;
+    double* x_new = op->xvec.p;
     cudaStream_t s = ctx->stream;
+    GEO_CHECK_ARG(o.use_preconditioner, "the matrix-free solver is Jacobi-preconditioned only");
     const bool mixed = o.precision == GEO_PRECISION_MIXED;
     const int64_t n = op->ndof;
-    int nb = op->pcg_blocks[0][mixed ? 1 : 0];
-    op->sc.ensure(nb);
-    // workspace: FP64 r, p, q (FP64 mode) or w (mixed); FP32 xs, r, p, q (mixed)
-    op->w64.ensure((size_t)3 * n);
-    if (mixed) op->w32.ensure((size_t)4 * n);
-    MfArgs a{};
-    a.pv = view(op);
-    a.qd64 = op->qd64.p;
-    a.qd32 = op->qd32.p;
-    a.cl = op->cl;
-    a.cm = op->cm;
-    a.cd = op->cd;
-    a.ndof = n;
-    a.b = b_new;
-    a.x64 = x_new;
-    a.r64 = op->w64.p;
-    a.p64 = op->w64.p + n;
-    a.q64 = op->w64.p + 2 * n;
-    a.w64 = op->w64.p;
-    a.dinv64 = op->dinv64.p;
-    a.dinv32 = op->dinv32.p;
-    if (mixed) {
-        a.xs = op->w32.p;
-        a.r32 = op->w32.p + n;
-        a.p32 = op->w32.p + 2 * n;
-        a.q32 = op->w32.p + 3 * n;
-        GEO_CUDA(cudaMemsetAsync(a.q32, 0, n * sizeof(float), s));
-        GEO_CUDA(cudaMemsetAsync(a.w64, 0, n * sizeof(double), s));
+    // workspace: FP64 mode: r, q, p0, p1 (double); mixed: w64 (double) + xs, r, q, p0, p1 (float)
+    op->w64.ensure((size_t)(mixed ? 1 : 4) * n);
+    if (mixed) op->w32.ensure((size_t)5 * n);
+    PcgState init{};
+    init.tol = o.tolerance;
+    init.abs_tol = o.abs_tolerance;
+    init.delta = o.reliable_delta;
+    init.cd = op->cd;
+    init.max_it = o.max_iterations;
+    GEO_CUDA(cudaMemcpyAsync(op->state.p, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    NodeArgs<double> n64{};
+    NodeArgs<float> n32{};
+    PatchArgs<double> p64{};
+    PatchArgs<float> p32{};
+    n64.flags = n32.flags = op->flags.p;
+    n64.n = n32.n = n;
+    n64.dpn = n32.dpn = op->dpn;
+    n64.st = n32.st = p64.st = p32.st = op->state.p;
+    p64.err = p32.err = &op->state.p->err;
+    n64.part = n32.part = op->part.p;
+    p64.part = p32.part = op->part.p + op->node_grid * 0;  // patch and node kernels never overlap
+    n64.b = n32.b = b_new;
+    n64.x64 = n32.x64 = x_new;
+    if (!mixed) {
+        n64.x = x_new;
+        n64.r = op->w64.p;
+        n64.q = op->w64.p + n;
+        n64.pbuf0 = op->w64.p + 2 * n;
+        n64.pbuf1 = op->w64.p + 3 * n;
+        n64.dinv = op->dinv64.p;
+        p64.r = n64.r;
+        p64.dinv = n64.dinv;
+        p64.pbuf0 = n64.pbuf0;
+        p64.pbuf1 = n64.pbuf1;
+        p64.y = n64.q;
     } else {
-        GEO_CUDA(cudaMemsetAsync(a.q64, 0, n * sizeof(double), s));
+        n32.w64 = op->w64.p;
+        n32.x = op->w32.p;
+        n32.r = op->w32.p + n;
+        n32.q = op->w32.p + 2 * n;
+        n32.pbuf0 = op->w32.p + 3 * n;
+        n32.pbuf1 = op->w32.p + 4 * n;
+        n32.dinv = op->dinv32.p;
+        p32.r = n32.r;
+        p32.dinv = n32.dinv;
+        p32.pbuf0 = n32.pbuf0;
+        p32.pbuf1 = n32.pbuf1;
+        p32.y = n32.q;
     }
-    a.part_a = op->sc.slot(0, nb);
-    a.part_b = op->sc.slot(1, nb);
-    a.part_c = op->sc.slot(2, nb);
-    a.gs = op->sc.gs.p;
-    a.res = op->sc.res.p;
-    a.timeout_ns = (unsigned long long)(o.timeout_seconds * 1e9);
-    a.max_it = o.max_iterations;
-    a.tol = o.tolerance;
-    a.abs_tol = o.abs_tolerance;
-    a.delta = o.reliable_delta;
-    GEO_CHECK_ARG(o.use_preconditioner, "the matrix-free solver is Jacobi-preconditioned only");
-    GEO_CUDA(cudaMemsetAsync(op->sc.gs.p, 0, sizeof(GridSync), s));
-    GEO_CUDA(cudaMemsetAsync(op->sc.res.p, 0, sizeof(PcgResult), s));
-    const size_t smem = smem_bytes(op, 8);
+    const unsigned ng = (unsigned)op->node_grid;
     GEO_CUDA(cudaEventRecord(ctx->ev0, s));
-    with_kernels(op, [&](auto k64, auto k32) {
-        using K64 = decltype(k64);
-        using K32 = decltype(k32);
-        if (mixed) launch_persistent(ctx, k_mf_pcg<K64, K32, true>, kMfBS, smem, a, nb);
-        else launch_persistent(ctx, k_mf_pcg<K64, K32, false>, kMfBS, smem, a, nb);
-    });
+    if (mixed) {
+        k_mixed_init1<<<ng, kNodeBS, 0, s>>>(n32);
+        k_mixed_init2<<<ng, kNodeBS, 0, s>>>(n32);
+    } else {
+        k_pcg_init<double><<<ng, kNodeBS, 0, s>>>(n64);
+    }
+    check_launch(ctx, "pcg init");
+    // (re)build the chunk graph when the buffers it captured changed
+    const int pi = mixed ? 1 : 0;
+    const void* key0 = mixed ? (const void*)op->w32.p : (const void*)op->w64.p;
+    const void* key1 = (const void*)x_new;
+    if (!op->chunk[pi] || op->chunk_key[pi][0] != key0 || op->chunk_key[pi][1] != key1) {
+        if (op->chunk[pi]) cudaGraphExecDestroy(op->chunk[pi]);
+        op->chunk[pi] = nullptr;
+        cudaGraph_t g;
+        GEO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        with_kernels(op, [&](auto k64, auto k32) {
+            for (int i = 0; i < kChunk; ++i) {
+                if (mixed) enqueue_iteration<decltype(k32), float, true>(op, s, p32, n32);
+                else enqueue_iteration<decltype(k64), double, false>(op, s, p64, n64);
+            }
+        });
+        GEO_CUDA(cudaStreamEndCapture(s, &g));
+        GEO_CUDA(cudaGraphInstantiate(&op->chunk[pi], g, 0));
+        cudaGraphDestroy(g);
+        op->chunk_key[pi][0] = key0;
+        op->chunk_key[pi][1] = key1;
+    }
+    long long launches = mixed ? 2 : 1;
+    const long long max_rounds = o.max_iterations / 1 + 64;
+    for (long long round = 0; round <= max_rounds; ++round) {
+        GEO_CUDA(cudaGraphLaunch(op->chunk[pi], s));
+        launches += 2 * kChunk;
+        GEO_CUDA(cudaMemcpyAsync(op->h_state, op->state.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+        sync(ctx, "PCG chunk");
+        if (op->h_state->err) fail(GEO_ERR_TIMEOUT, "matrix-free PCG: a bounded device-side wait timed out");
+        if (op->h_state->flags & ST_DONE) break;
+        if (mixed && (op->h_state->flags & ST_REFRESH)) {
+            PatchArgs<double> ra{};
+            ra.x = x_new;
+            ra.y = op->w64.p;
+            ra.err = &op->state.p->err;
+            k_refresh_flush<<<ng, kNodeBS, 0, s>>>(n32);
+            with_kernels(op, [&](auto k64, auto) {
+                launch_patch<decltype(k64), double, MODE_FREE>(op, 0, s, op->qd64.p, ra);
+            });
+            k_refresh_residual<<<ng, kNodeBS, 0, s>>>(n32);
+            k_refresh_rescale<<<ng, kNodeBS, 0, s>>>(n32);
+            check_launch(ctx, "refresh");
+            launches += 4;
+            GEO_CUDA(cudaMemcpyAsync(op->h_state, op->state.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+            sync(ctx, "refresh");
+            if (op->h_state->err) fail(GEO_ERR_TIMEOUT, "matrix-free PCG: a bounded device-side wait timed out");
+            if (op->h_state->flags & ST_DONE) break;
+        }
+    }
+    if (mixed && !(op->h_state->flags & ST_CONVERGED)) {
+        k_refresh_flush<<<ng, kNodeBS, 0, s>>>(n32);  // keep the FP32 correction
+        check_launch(ctx, "final flush");
+        launches += 1;
+    }
     GEO_CUDA(cudaEventRecord(ctx->ev1, s));
-    PcgResult r{};
-    GridSync g{};
-    GEO_CUDA(cudaMemcpyAsync(&r, op->sc.res.p, sizeof(r), cudaMemcpyDeviceToHost, s));
-    GEO_CUDA(cudaMemcpyAsync(&g, op->sc.gs.p, sizeof(g), cudaMemcpyDeviceToHost, s));
     sync(ctx, "matrix-free PCG");
     float ms = 0.f;
     GEO_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    if (g.error & DEV_ERR_TIMEOUT) {
-        fill_stats(st, r, ms * 1e-3, GEO_ERR_TIMEOUT);
-        fail(GEO_ERR_TIMEOUT, "PCG grid barrier timed out");
-    }
+    const PcgState& h = *op->h_state;
+    PcgResult r{h.it, h.res, h.bnorm, (h.flags & ST_CONVERGED) ? 1 : 0, (h.flags & ST_BREAKDOWN) ? 1 : 0, h.nupd};
     const int status = r.converged ? GEO_OK : (r.breakdown ? GEO_ERR_BREAKDOWN : GEO_NOT_CONVERGED);
     fill_stats(st, r, ms * 1e-3, status);
+    if (st) st->kernel_launches = launches;
     return status;
 }
 
@@ -1041,12 +840,17 @@ int geo_cg_solve_matfree(geo_op* op, const double* b, const geo_cg_opts* opts, d
     cg_opts_fill(opts, o);
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
-    DevBuf<double> tb, bn(n), xn(n), xo(n);
+    DevBuf<double> tb, xo;
     const double* db = stage_in(b, n, tb, s);
-    to_new(op, db, bn.p);
-    const int status = solve_new(op, bn.p, o, xn.p, st);
-    to_orig(op, xn.p, xo.p);
-    copy_out(x, xo.p, n, s);
+    to_new(op, db, op->bvec.p);
+    const int status = solve_new(op, o, st);
+    double* dst = x;
+    if (!is_device_ptr(x)) {
+        xo.alloc(n);
+        dst = xo.p;
+    }
+    to_orig(op, op->xvec.p, dst);
+    if (dst != x) copy_out(x, dst, n, s);
     sync(op->ctx, "geo_cg_solve_matfree");
     return finish_status(op->ctx, status);
     GEO_API_END
@@ -1076,12 +880,17 @@ int geo_forward(geo_op* op, const double* f, const geo_cg_opts* opts, double* u,
     cg_opts_fill(opts, o);
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
-    DevBuf<double> tf, fb(n), xn(n), xo(n);
+    DevBuf<double> tf, xo;
     const double* df = stage_in(f, n, tf, s);
-    lift_new(op, df, fb.p);
-    const int status = solve_new(op, fb.p, o, xn.p, st);
-    to_orig(op, xn.p, xo.p);
-    copy_out(u, xo.p, n, s);
+    lift_new(op, df, op->bvec.p);
+    const int status = solve_new(op, o, st);
+    double* dst = u;
+    if (!is_device_ptr(u)) {
+        xo.alloc(n);
+        dst = xo.p;
+    }
+    to_orig(op, op->xvec.p, dst);
+    if (dst != u) copy_out(u, dst, n, s);
     sync(op->ctx, "geo_forward");
     return finish_status(op->ctx, status);
     GEO_API_END
@@ -1095,28 +904,28 @@ int geo_vjp(geo_op* op, const double* f, const double* u, const double* dJ_du, c
     cg_opts_fill(opts, o);
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
-    DevBuf<double> tu, tg, uo(n), gn(n), ln(n), lo(n), ge(op->E);
+    DevBuf<double> tu, tg, uo(n), lo(n), ge(op->E);
     const double* du = nullptr;
     if (u) {
         du = stage_in(u, n, tu, s);
     } else {
         // recompute the forward solution instead of storing it
-        DevBuf<double> tf, fb(n), xn(n);
+        DevBuf<double> tf;
         const double* df = stage_in(f, n, tf, s);
-        lift_new(op, df, fb.p);
-        const int fs = solve_new(op, fb.p, o, xn.p, nullptr);
+        lift_new(op, df, op->bvec.p);
+        const int fs = solve_new(op, o, nullptr);
         if (fs != GEO_OK) return finish_status(op->ctx, fs);
-        to_orig(op, xn.p, uo.p);
+        to_orig(op, op->xvec.p, uo.p);
         du = uo.p;
     }
     // adjoint right-hand side: dJ/du on free DOFs, zero on Dirichlet DOFs (K_bc
     // is symmetric and its Dirichlet rows are decoupled, so lambda_D = 0)
     const double* dg = stage_in(dJ_du, n, tg, s);
-    to_new(op, dg, gn.p);
-    k_zero_dir<double><<<nblk(n), 256, 0, s>>>(op->flags.p, op->dpn, n, gn.p);
+    to_new(op, dg, op->bvec.p);
+    k_zero_dir<double><<<nblk(n), 256, 0, s>>>(op->flags.p, op->dpn, n, op->bvec.p);
     check_launch(op->ctx, "adjoint rhs");
-    const int status = solve_new(op, gn.p, o, ln.p, st);
-    to_orig(op, ln.p, lo.p);
+    const int status = solve_new(op, o, st);
+    to_orig(op, op->xvec.p, lo.p);
     const geo_mesh* m = op->mesh;
     k_elem_gradient<<<(unsigned)cdiv(op->E, 128), 128, 0, s>>>(op->phys, m->xyz.p, m->conn.p, op->N, op->E,
                                                                op->coef.p, op->cl, op->cm, op->mask_orig.p, du,

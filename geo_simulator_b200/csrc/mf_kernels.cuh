@@ -1,0 +1,601 @@
+// Kernels of the matrix-free operator and its PCG (see matfree.cu).
+//
+// Patch apply (k_patch): a CTA works through whole patches (patch = blockIdx.x,
+// += gridDim.x). The patch's element data (16-bit local connectivity and the
+// per-element qdata, contiguous per patch) is brought into shared memory with
+// cp.async.bulk (bulk copy engine, mbarrier completion), double-buffered so the
+// next patch's copy is in flight while the current one is processed. Per patch:
+//   1. gather: every patch-local node's input value is read once from global
+//      memory into a shared table (own nodes form one contiguous range);
+//   2. element pass: each thread applies K_e to its elements from the shared
+//      table and accumulates into a shared output table with shared atomics.
+//      Elements are ordered so a warp's 32 elements share no node, so these
+//      atomics do not collide;
+//   3. flush: a plain store for nodes no other patch touches, red.global.add
+//      for the shared ones.
+// In PCG mode step 1 also forms the new search direction p = z + beta p_old
+// (z = D^-1 r) on the fly: the Jacobi scaling and the p-update ride on the
+// operator's gather. p is double-buffered by iteration parity.
+//
+// PCG node update (k_pcg_update): x += alpha p, r -= alpha q (Dirichlet rows
+// q = char_diag p), z = D^-1 r, and the r.r / r.z partial sums; loads are
+// issued for several entries before any store so they overlap.
+//
+// Every reduction is single pass: each block writes its partial, the last block
+// to finish (ticket counter) sums the partials in a fixed order and updates the
+// device-resident PcgState, which the next kernel reads. No host round trip per
+// iteration and no grid-wide spin wait.
+#pragma once
+
+#include "matfree.cuh"
+#include "patches.h"
+
+namespace geo {
+
+constexpr int kPatchBS = 192;  // threads of the patch kernel (2 elements each)
+constexpr int kNodeBS = 256;   // threads of the node kernels
+constexpr int kUnroll = 4;     // entries in flight per thread in the node kernels
+constexpr int kGather = 4;     // patch-local nodes in flight per thread in the gather
+
+enum : int { MODE_FREE = 0, MODE_LIFT = 1, MODE_PCG = 2 };
+enum : int { ST_DONE = 1, ST_REFRESH = 2, ST_CONVERGED = 4, ST_BREAKDOWN = 8 };
+enum : int { TICKET_PATCH = 0, TICKET_UPDATE = 1, TICKET_AUX = 2 };
+
+struct PatchView {
+    int64_t E, N;
+    int n_patches, max_local, dpn;
+    const int32_t* pe;
+    const int32_t* po;
+    const int32_t* pf;
+    const int32_t* foreign;
+    const uint32_t* lc;  // patch-major paired connectivity [P][5][kPatchElems]
+    const uint8_t* flags;
+};
+
+// Device-resident PCG scalars.
+struct PcgState {
+    double rz, rz_old, pAp, alpha, beta, bnorm, s_scale, rmax, res, ratio, s_new;
+    double tol, abs_tol, delta, cd;
+    long long it, max_it, nupd;
+    int flags;
+    int err;  // DEV_ERR_* bits raised by bounded waits
+    unsigned int ticket[4];
+};
+
+template <class T>
+struct PatchArgs {
+    const T* x;  // FREE / LIFT input
+    T* y;        // output (free rows)
+    // PCG mode
+    const T* r;
+    const T* dinv;
+    T* pbuf0;
+    T* pbuf1;
+    PcgState* st;
+    double* part;  // [gridDim.x][2]
+    int* err;      // DEV_ERR_* bits (bounded waits)
+};
+
+// ------------------------------------------------------------------ bulk copy + mbarrier
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// global -> shared bulk copy (no multicast); dst/src 16-byte aligned, bytes % 16 == 0
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait (2 s of %globaltimer); returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_timer_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_timer_ns() - t0 > 2000000000ull) return false;
+    return true;
+}
+
+// Last-block detection after every block stored its partial.
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last != 0;
+}
+
+// bytes of one patch's element data (connectivity + qdata), 16-byte multiple
+template <class K, class T>
+__host__ __device__ constexpr uint32_t patch_bytes_lc() { return 5 * kPatchElems * 4; }
+template <class K, class T>
+__host__ __device__ constexpr uint32_t patch_bytes_qd() { return K::NQD * kPatchElems * (uint32_t)sizeof(T); }
+
+// shared memory layout: [2 mbarriers | NBUF x (lc | qd) | xs | ys | node ids | flags]
+template <class K, class T, int NBUF>
+__host__ __device__ constexpr size_t patch_smem_fixed() {
+    return 16 + (size_t)NBUF * (patch_bytes_lc<K, T>() + patch_bytes_qd<K, T>());
+}
+
+template <class K, class T, int MODE, int NBUF>
+__global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __restrict__ qd_all, T cl, T cm,
+                                                    PatchArgs<T> a) {
+    constexpr int DPN = K::DPN;
+    constexpr uint32_t LCB = patch_bytes_lc<K, T>(), QDB = patch_bytes_qd<K, T>();
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    unsigned char* ebuf = smem + 16;
+    T* xs = reinterpret_cast<T*>(smem + patch_smem_fixed<K, T, NBUF>());
+    T* ys = xs + (size_t)pv.max_local * DPN;
+    int* snode = reinterpret_cast<int*>(ys + (size_t)pv.max_local * DPN);
+    uint8_t* sfl = reinterpret_cast<uint8_t*>(snode + pv.max_local);
+    T beta = T(0);
+    const T* pold = nullptr;
+    T* pnew = nullptr;
+    if (MODE == MODE_PCG) {
+        if (a.st->flags & (ST_DONE | ST_REFRESH)) return;
+        beta = (T)a.st->beta;
+        const bool odd = a.st->it & 1;
+        pold = odd ? a.pbuf1 : a.pbuf0;
+        pnew = odd ? a.pbuf0 : a.pbuf1;
+    }
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NBUF; ++b) mbar_init(&bar[b], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](int patch, int b) {
+        unsigned char* dst = ebuf + (size_t)b * (LCB + QDB);
+        mbar_expect_tx(&bar[b], LCB + QDB);
+        bulk_g2s(dst, pv.lc + (size_t)patch * 5 * kPatchElems, LCB, &bar[b]);
+        bulk_g2s(dst + LCB, qd_all + (size_t)patch * K::NQD * kPatchElems, QDB, &bar[b]);
+    };
+    if (threadIdx.x == 0 && blockIdx.x < pv.n_patches) issue(blockIdx.x, 0);
+    uint32_t phase = 0;  // bit b = parity of buffer b
+    double dot = 0.0, pdd = 0.0;
+    int k = 0;
+    for (int patch = blockIdx.x; patch < pv.n_patches; patch += gridDim.x, ++k) {
+        const int b = NBUF == 2 ? (k & 1) : 0;
+        if (NBUF == 2 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, b ^ 1);
+        const int e0 = pv.pe[patch], n_el = pv.pe[patch + 1] - e0;
+        const int o0 = pv.po[patch], nown = pv.po[patch + 1] - o0;
+        const int f0 = pv.pf[patch], nloc = nown + pv.pf[patch + 1] - f0;
+        // 1. gather (overlaps the bulk copies in flight); each thread issues the
+        //    loads of up to kGather nodes before any store
+        for (int u0 = threadIdx.x; u0 < nloc; u0 += kGather * blockDim.x) {
+            int node[kGather];
+            uint8_t fl[kGather];
+            T d0[kGather][DPN], d1[kGather][DPN], d2[kGather][DPN];
+#pragma unroll
+            for (int g = 0; g < kGather; ++g) {
+                const int u = u0 + g * blockDim.x;
+                node[g] = u < nown ? o0 + u : (u < nloc ? pv.foreign[f0 + u - nown] : 0);
+            }
+#pragma unroll
+            for (int g = 0; g < kGather; ++g) {
+                const int u = u0 + g * blockDim.x;
+                if (u < nloc) {
+                    fl[g] = pv.flags[node[g]];
+#pragma unroll
+                    for (int c = 0; c < DPN; ++c) {
+                        const int64_t idx = (int64_t)node[g] * DPN + c;
+                        if (MODE == MODE_PCG) {
+                            d0[g][c] = a.dinv[idx];
+                            d1[g][c] = a.r[idx];
+                            d2[g][c] = pold[idx];
+                        } else {
+                            d0[g][c] = a.x[idx];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < kGather; ++g) {
+                const int u = u0 + g * blockDim.x;
+                if (u >= nloc) continue;
+                snode[u] = node[g];
+                sfl[u] = fl[g];
+#pragma unroll
+                for (int c = 0; c < DPN; ++c) {
+                    const bool dir = (fl[g] >> c) & 1;
+                    T v;
+                    if (MODE == MODE_PCG) {
+                        const T pn = d0[g][c] * d1[g][c] + beta * d2[g][c];
+                        if (u < nown) {
+                            pnew[(int64_t)node[g] * DPN + c] = pn;
+                            if (dir) pdd += (double)(pn * pn);
+                        }
+                        v = dir ? T(0) : pn;
+                    } else {
+                        v = d0[g][c];
+                        if (MODE == MODE_FREE ? dir : !dir) v = T(0);
+                    }
+                    xs[u * DPN + c] = v;
+                    ys[u * DPN + c] = T(0);
+                }
+            }
+        }
+        const bool ok = mbar_wait(&bar[b], (phase >> b) & 1);
+        phase ^= 1u << b;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(a.err, DEV_ERR_TIMEOUT);
+            return;
+        }
+        // 2. elements
+        const uint32_t* lcs = reinterpret_cast<const uint32_t*>(ebuf + (size_t)b * (LCB + QDB));
+        const T* qds = reinterpret_cast<const T*>(ebuf + (size_t)b * (LCB + QDB) + LCB);
+        for (int el = threadIdx.x; el < n_el; el += blockDim.x) {
+            int li[10];
+            T xe[10 * DPN], ye[10 * DPN];
+#pragma unroll
+            for (int l2 = 0; l2 < 5; ++l2) {
+                const uint32_t w = lcs[l2 * kPatchElems + el];
+                li[2 * l2] = (int)(w & 0xffffu);
+                li[2 * l2 + 1] = (int)(w >> 16);
+            }
+#pragma unroll
+            for (int l = 0; l < 10; ++l)
+#pragma unroll
+                for (int c = 0; c < DPN; ++c) xe[l * DPN + c] = xs[li[l] * DPN + c];
+            K::apply(qds + el, kPatchElems, cl, cm, xe, ye);
+            if (MODE == MODE_PCG) {
+                T d = T(0);
+#pragma unroll
+                for (int q = 0; q < 10 * DPN; ++q) d += xe[q] * ye[q];
+                dot += (double)d;
+            }
+#pragma unroll
+            for (int l = 0; l < 10; ++l)
+#pragma unroll
+                for (int c = 0; c < DPN; ++c) atomicAdd(&ys[li[l] * DPN + c], ye[l * DPN + c]);
+        }
+        __syncthreads();
+        if (NBUF == 1 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, 0);
+        // 3. flush
+        for (int u = threadIdx.x; u < nloc; u += blockDim.x) {
+            const int node = snode[u];
+            const uint8_t fl = sfl[u];
+            const bool plain = u < nown && !(fl & kFlagShared);
+#pragma unroll
+            for (int c = 0; c < DPN; ++c) {
+                if ((fl >> c) & 1) continue;
+                const T v = ys[u * DPN + c];
+                T* dst = a.y + (int64_t)node * DPN + c;
+                if (plain) *dst = v;
+                else atomicAdd(dst, v);
+            }
+        }
+        __syncthreads();
+    }
+    if (MODE == MODE_PCG) {
+        double v[2] = {dot, pdd};
+        store_partial<2>(a.part, v);
+        if (last_block(&a.st->ticket[TICKET_PATCH])) {
+            double t[2];
+            grid_total<2>(a.part, gridDim.x, t);
+            if (threadIdx.x == 0) {
+                PcgState* st = a.st;
+                st->ticket[TICKET_PATCH] = 0;
+                const double pAp = t[0] + st->cd * t[1];
+                st->pAp = pAp;
+                if (fabs(pAp) < 1e-30) {  // iterative.rs:85
+                    st->flags |= ST_DONE | ST_BREAKDOWN;
+                } else {
+                    st->alpha = st->rz / pAp;
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ node kernels
+template <class T>
+struct NodeArgs {
+    const uint8_t* flags;
+    int64_t n;
+    int dpn;
+    T* x;  // solution (FP64 mode) or FP32 correction xs (mixed)
+    T* r;
+    T* q;
+    const T* dinv;
+    T* pbuf0;
+    T* pbuf1;
+    PcgState* st;
+    double* part;
+    // mixed refresh
+    double* x64;
+    double* w64;
+    const double* b;
+};
+
+// x += alpha p, r -= alpha q, z = D^-1 r; r.r and r.z; stopping / refresh decision.
+template <class T, int DPN, bool MIXED>
+__global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
+    PcgState* st = a.st;
+    if (st->flags & (ST_DONE | ST_REFRESH)) return;
+    const T alpha = (T)st->alpha;
+    const T cd = (T)st->cd;
+    const T* __restrict__ p = (st->it & 1) ? a.pbuf0 : a.pbuf1;
+    const uint8_t* __restrict__ flags = a.flags;
+    const T* __restrict__ dinv = a.dinv;
+    T* __restrict__ x = a.x;
+    T* __restrict__ r = a.r;
+    T* __restrict__ q = a.q;
+    const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
+    T acc_rr = T(0), acc_rz = T(0);
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; i + (kUnroll - 1) * nth < n; i += kUnroll * nth) {
+        uint8_t fl[kUnroll];
+        T pj[kUnroll], qj[kUnroll], xj[kUnroll], rj[kUnroll], dj[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int64_t j = i + u * nth;
+            fl[u] = flags[j / DPN];
+            pj[u] = p[j];
+            qj[u] = q[j];
+            xj[u] = x[j];
+            rj[u] = r[j];
+            dj[u] = dinv[j];
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int64_t j = i + u * nth;
+            const bool dir = (fl[u] >> (j % DPN)) & 1;
+            const T qq = dir ? cd * pj[u] : qj[u];
+            if (!dir && (fl[u] & kFlagShared)) q[j] = T(0);
+            x[j] = xj[u] + alpha * pj[u];
+            const T rr = rj[u] - alpha * qq;
+            r[j] = rr;
+            acc_rr += rr * rr;
+            acc_rz += rr * (rr * dj[u]);
+        }
+    }
+    for (; i < n; i += nth) {
+        const uint8_t f = flags[i / DPN];
+        const bool dir = (f >> (i % DPN)) & 1;
+        const T pj = p[i];
+        const T qq = dir ? cd * pj : q[i];
+        if (!dir && (f & kFlagShared)) q[i] = T(0);
+        x[i] += alpha * pj;
+        const T rr = r[i] - alpha * qq;
+        r[i] = rr;
+        acc_rr += rr * rr;
+        acc_rz += rr * (rr * dinv[i]);
+    }
+    double v[2] = {(double)acc_rr, (double)acc_rz};
+    store_partial<2>(a.part, v);
+    if (last_block(&st->ticket[TICKET_UPDATE])) {
+        double t[2];
+        grid_total<2>(a.part, gridDim.x, t);
+        if (threadIdx.x == 0) {
+            st->ticket[TICKET_UPDATE] = 0;
+            const double rn = sqrt(t[0]);
+            if (!MIXED) {
+                st->res = rn;
+                if (rn < st->tol * st->bnorm || rn < st->abs_tol) {  // iterative.rs:95
+                    st->flags |= ST_DONE | ST_CONVERGED;
+                    return;
+                }
+            }
+            st->beta = t[1] / st->rz;
+            st->rz_old = st->rz;
+            st->rz = t[1];
+            st->it += 1;
+            if (MIXED) {
+                st->rmax = fmax(st->rmax, rn);
+                const double est = rn * st->s_scale;
+                if (est < st->tol * st->bnorm || est < st->abs_tol || rn < st->delta * st->rmax ||
+                    st->it >= st->max_it)
+                    st->flags |= ST_REFRESH;
+            } else if (st->it >= st->max_it) {
+                st->flags |= ST_DONE;
+            }
+        }
+    }
+}
+
+// FP64 mode start: x = 0, r = b, p_old = 0, q = 0; ||b||, r.z.
+template <class T>
+__global__ void __launch_bounds__(kNodeBS) k_pcg_init(NodeArgs<T> a) {
+    const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
+    double bb = 0.0, rz = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += nth) {
+        const double bi = a.b[i];
+        a.x[i] = T(0);
+        a.r[i] = (T)bi;
+        a.q[i] = T(0);
+        a.pbuf0[i] = T(0);
+        bb += bi * bi;
+        rz += bi * (bi * (double)a.dinv[i]);
+    }
+    double v[2] = {bb, rz};
+    store_partial<2>(a.part, v);
+    if (last_block(&a.st->ticket[TICKET_AUX])) {
+        double t[2];
+        grid_total<2>(a.part, gridDim.x, t);
+        if (threadIdx.x == 0) {
+            PcgState* st = a.st;
+            st->ticket[TICKET_AUX] = 0;
+            st->bnorm = sqrt(t[0]);
+            st->res = st->bnorm;
+            st->rz = t[1];
+            st->beta = 0.0;
+            st->it = 0;
+            st->nupd = 0;
+            st->s_scale = 1.0;
+            st->rmax = 1.0;
+            if (st->bnorm < 1e-25) {  // iterative.rs:60-68
+                st->flags |= ST_DONE | ST_CONVERGED;
+                st->res = 0.0;
+            }
+            if (st->max_it <= 0) st->flags |= ST_DONE;
+        }
+    }
+}
+
+// MIXED start, pass 1: x64 = 0, xs = 0, q = 0, w64 = 0, p_old = 0; ||b||.
+__global__ void __launch_bounds__(kNodeBS) k_mixed_init1(NodeArgs<float> a) {
+    const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
+    double bb = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += nth) {
+        const double bi = a.b[i];
+        a.x64[i] = 0.0;
+        a.w64[i] = 0.0;
+        a.x[i] = 0.0f;
+        a.q[i] = 0.0f;
+        a.pbuf0[i] = 0.0f;
+        bb += bi * bi;
+    }
+    double v[1] = {bb};
+    store_partial<1>(a.part, v);
+    if (last_block(&a.st->ticket[TICKET_AUX])) {
+        double t[1];
+        grid_total<1>(a.part, gridDim.x, t);
+        if (threadIdx.x == 0) {
+            PcgState* st = a.st;
+            st->ticket[TICKET_AUX] = 0;
+            st->bnorm = sqrt(t[0]);
+            st->res = st->bnorm;
+            st->s_scale = st->bnorm;
+            st->beta = 0.0;
+            st->it = 0;
+            st->nupd = 0;
+            st->rmax = 1.0;
+            if (st->bnorm < 1e-25) {
+                st->flags |= ST_DONE | ST_CONVERGED;
+                st->res = 0.0;
+            }
+            if (st->max_it <= 0) st->flags |= ST_DONE;
+        }
+    }
+}
+
+// MIXED start, pass 2: r = b / ||b|| (FP32), r.z.
+__global__ void __launch_bounds__(kNodeBS) k_mixed_init2(NodeArgs<float> a) {
+    if (a.st->flags & ST_DONE) return;
+    const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
+    const double inv = 1.0 / a.st->s_scale;
+    double rz = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += nth) {
+        const float ri = (float)(a.b[i] * inv);
+        a.r[i] = ri;
+        rz += (double)(ri * (ri * a.dinv[i]));
+    }
+    double v[1] = {rz};
+    store_partial<1>(a.part, v);
+    if (last_block(&a.st->ticket[TICKET_AUX])) {
+        double t[1];
+        grid_total<1>(a.part, gridDim.x, t);
+        if (threadIdx.x == 0) {
+            a.st->ticket[TICKET_AUX] = 0;
+            a.st->rz = t[0];
+        }
+    }
+}
+
+// MIXED refresh 1: x64 += s xs, xs = 0.
+__global__ void __launch_bounds__(kNodeBS) k_refresh_flush(NodeArgs<float> a) {
+    const double s = a.st->s_scale;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        a.x64[i] += s * (double)a.x[i];
+        a.x[i] = 0.0f;
+    }
+}
+
+// MIXED refresh 3: w = b - K_bc x64 (w holds K x64 on free rows); ||w|| decides
+// convergence (FP64 true residual).
+__global__ void __launch_bounds__(kNodeBS) k_refresh_residual(NodeArgs<float> a) {
+    PcgState* st = a.st;
+    const double cd = st->cd;
+    double rr = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const bool dir = (a.flags[i / a.dpn] >> (i % a.dpn)) & 1;
+        const double kx = dir ? cd * a.x64[i] : a.w64[i];
+        const double ri = a.b[i] - kx;
+        a.w64[i] = ri;
+        rr += ri * ri;
+    }
+    double v[1] = {rr};
+    store_partial<1>(a.part, v);
+    if (last_block(&st->ticket[TICKET_AUX])) {
+        double t[1];
+        grid_total<1>(a.part, gridDim.x, t);
+        if (threadIdx.x == 0) {
+            st->ticket[TICKET_AUX] = 0;
+            const double s_new = sqrt(t[0]);
+            st->nupd += 1;
+            st->res = s_new;
+            st->s_new = s_new;
+            if (s_new < st->tol * st->bnorm || s_new < st->abs_tol) {
+                st->flags = (st->flags & ~ST_REFRESH) | ST_DONE | ST_CONVERGED;
+            } else {
+                st->ratio = st->s_scale / s_new;
+            }
+        }
+    }
+}
+
+// MIXED refresh 4: r = w / ||w||, current p rescaled, r.z recomputed.
+__global__ void __launch_bounds__(kNodeBS) k_refresh_rescale(NodeArgs<float> a) {
+    PcgState* st = a.st;
+    if (st->flags & ST_DONE) return;
+    const double inv = 1.0 / st->s_new;
+    const float ratio = (float)st->ratio;
+    float* p = (st->it & 1) ? a.pbuf1 : a.pbuf0;  // direction the next apply reads
+    double rz = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t fl = a.flags[i / a.dpn];
+        const double wi = a.w64[i];
+        if (!((fl >> (i % a.dpn)) & 1) && (fl & kFlagShared)) a.w64[i] = 0.0;
+        const float ri = (float)(wi * inv);
+        a.r[i] = ri;
+        p[i] *= ratio;
+        rz += (double)(ri * (ri * a.dinv[i]));
+    }
+    double v[1] = {rz};
+    store_partial<1>(a.part, v);
+    if (last_block(&st->ticket[TICKET_AUX])) {
+        double t[1];
+        grid_total<1>(a.part, gridDim.x, t);
+        if (threadIdx.x == 0) {
+            st->ticket[TICKET_AUX] = 0;
+            const double ratio2 = st->ratio * st->ratio;
+            st->beta = t[0] / (st->rz_old * ratio2);
+            st->rz = t[0];
+            st->s_scale = st->s_new;
+            st->rmax = 1.0;
+            st->flags &= ~ST_REFRESH;
+            if (st->it >= st->max_it) st->flags |= ST_DONE;
+        }
+    }
+}
+
+// y_D = cd x_D after a MODE_FREE pass
+template <class T>
+__global__ void k_dir_rows(const uint8_t* flags, int dpn, int64_t n, double cd, const T* x, T* y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if ((flags[i / dpn] >> (i % dpn)) & 1) y[i] = (T)(cd * (double)x[i]);
+}
+
+}  // namespace geo

@@ -19,8 +19,6 @@ struct geo_ctx {
 struct geo_mesh {
     geo_ctx* ctx = nullptr;
     int64_t n_nodes = 0, n_elem = 0;
-    std::vector<double> h_xyz;     // AoS [N][3]
-    std::vector<int32_t> h_conn;   // AoS [E][10]
     geo::DevBuf<double> xyz;       // SoA [3][N]
     geo::DevBuf<int32_t> conn;     // SoA [10][E]
     // node -> (element*10 + local) incidence list sorted by element (built lazily)

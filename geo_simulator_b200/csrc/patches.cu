@@ -1,0 +1,375 @@
+// GPU construction of the element-patch layout (see patches.h). All steps are
+// data-parallel: Morton keys + radix sort for the element order, atomicMin of
+// the first-touch position for the node order, one 64-bit key sort for the
+// per-patch foreign lists, binary searches for the local indices.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+
+#include "patches.h"
+
+namespace geo {
+namespace {
+
+inline unsigned nb(int64_t n, int bs = 256) { return (unsigned)std::max<int64_t>(1, cdiv(n, bs)); }
+
+__device__ __forceinline__ uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void k_morton(const double* __restrict__ xyz, const int32_t* __restrict__ conn, int64_t N, int64_t E,
+                         const double* __restrict__ lohi, uint64_t* __restrict__ key, int32_t* __restrict__ idx) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    uint64_t q[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double cen = 0.0;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) cen += 0.25 * xyz[c * N + conn[v * E + e]];
+        const double lo = lohi[c], hi = lohi[3 + c];
+        const double sc = hi > lo ? (double)((1 << 21) - 1) / (hi - lo) : 0.0;
+        q[c] = (uint64_t)llrint(fmin(fmax((cen - lo) * sc, 0.0), (double)((1 << 21) - 1)));
+    }
+    key[e] = spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2;
+    idx[e] = (int32_t)e;
+}
+
+__global__ void k_bbox(const double* __restrict__ xyz, int64_t N, unsigned long long* __restrict__ out) {
+    // out[0..2] = ordered-int of min, out[3..5] = ordered-int of max
+    double lo[3] = {1e308, 1e308, 1e308}, hi[3] = {-1e308, -1e308, -1e308};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double v = xyz[c * N + i];
+            lo[c] = fmin(lo[c], v);
+            hi[c] = fmax(hi[c], v);
+        }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[c] = fmin(lo[c], __shfl_down_sync(0xffffffffu, lo[c], o));
+            hi[c] = fmax(hi[c], __shfl_down_sync(0xffffffffu, hi[c], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        // map doubles to order-preserving unsigned keys
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            unsigned long long a = (unsigned long long)__double_as_longlong(lo[c]);
+            a = (a >> 63) ? ~a : (a | 0x8000000000000000ull);
+            atomicMin(&out[c], a);
+            unsigned long long b = (unsigned long long)__double_as_longlong(hi[c]);
+            b = (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+            atomicMax(&out[3 + c], b);
+        }
+    }
+}
+
+__global__ void k_bbox_decode(const unsigned long long* in, double* lohi) {
+    const int c = threadIdx.x;
+    if (c >= 6) return;
+    unsigned long long a = in[c];
+    a = (a >> 63) ? (a & 0x7fffffffffffffffull) : ~a;
+    lohi[c] = __longlong_as_double((long long)a);
+}
+
+__global__ void k_first_touch(const int32_t* __restrict__ conn, const int32_t* __restrict__ eperm, int64_t E,
+                              int32_t* __restrict__ ft) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= E * 10) return;
+    const int64_t ne = t / 10;
+    const int l = (int)(t % 10);
+    atomicMin(&ft[conn[l * E + eperm[ne]]], (int32_t)t);
+}
+
+__global__ void k_fill_max(int32_t* v, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = INT_MAX;
+}
+
+__global__ void k_iota(int32_t* v, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (int32_t)i;
+}
+
+__global__ void k_inverse(const int32_t* __restrict__ perm, int64_t n, int32_t* __restrict__ inv) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) inv[perm[i]] = (int32_t)i;
+}
+
+// patch_elem[p] = min(p*PE, E); patch_own[p] = #new nodes with first touch < p*PE*10
+__global__ void k_patch_bounds(const int32_t* __restrict__ ft_sorted, int64_t N, int64_t E, int P,
+                               int32_t* __restrict__ pe, int32_t* __restrict__ po) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > P) return;
+    const int64_t e0 = std::min<int64_t>((int64_t)p * kPatchElems, E);
+    pe[p] = (int32_t)e0;
+    const int64_t key = e0 * 10;
+    int64_t lo = 0, hi = N;
+    while (lo < hi) {
+        const int64_t m = (lo + hi) >> 1;
+        if ((int64_t)ft_sorted[m] < key) lo = m + 1;
+        else hi = m;
+    }
+    po[p] = (int32_t)lo;
+}
+
+// key = patch << 32 | new node for every foreign incidence, ~0 otherwise
+__global__ void k_foreign_keys(const int32_t* __restrict__ conn, const int32_t* __restrict__ eperm,
+                               const int32_t* __restrict__ ninv, const int32_t* __restrict__ po, int64_t E,
+                               uint64_t* __restrict__ key) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= E * 10) return;
+    const int64_t ne = t / 10;
+    const int l = (int)(t % 10);
+    const int32_t nn = ninv[conn[l * E + eperm[ne]]];
+    const int p = (int)(ne / kPatchElems);
+    key[t] = nn < po[p] ? ((uint64_t)p << 32 | (uint32_t)nn) : ~0ull;
+}
+
+__global__ void k_foreign_bounds(const uint64_t* __restrict__ uniq, int64_t nf, int P, int32_t* __restrict__ pf) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > P) return;
+    const uint64_t key = (uint64_t)p << 32;
+    int64_t lo = 0, hi = nf;
+    while (lo < hi) {
+        const int64_t m = (lo + hi) >> 1;
+        if (uniq[m] < key) lo = m + 1;
+        else hi = m;
+    }
+    pf[p] = (int32_t)lo;
+}
+
+__global__ void k_foreign_nodes(const uint64_t* __restrict__ uniq, int64_t nf, int32_t* __restrict__ foreign,
+                                uint8_t* __restrict__ shared) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nf) return;
+    const int32_t nn = (int32_t)(uniq[j] & 0xffffffffull);
+    foreign[j] = nn;
+    shared[nn] = 1;
+}
+
+__global__ void k_local_conn(const int32_t* __restrict__ conn, const int32_t* __restrict__ eperm,
+                             const int32_t* __restrict__ ninv, const int32_t* __restrict__ po,
+                             const int32_t* __restrict__ pf, const int32_t* __restrict__ foreign, int64_t E,
+                             uint16_t* __restrict__ lconn, int* __restrict__ err) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= E * 10) return;
+    const int64_t ne = t / 10;
+    const int l = (int)(t % 10);
+    const int32_t nn = ninv[conn[l * E + eperm[ne]]];
+    const int p = (int)(ne / kPatchElems);
+    const int32_t own0 = po[p], nown = po[p + 1] - own0;
+    int64_t loc;
+    if (nn >= own0) {
+        loc = nn - own0;
+        if (loc >= nown) atomicOr(err, DEV_ERR_BOUNDS);
+    } else {
+        int64_t lo = pf[p], hi = pf[p + 1];
+        while (lo < hi) {
+            const int64_t m = (lo + hi) >> 1;
+            if (foreign[m] < nn) lo = m + 1;
+            else hi = m;
+        }
+        if (lo >= pf[p + 1] || foreign[lo] != nn) atomicOr(err, DEV_ERR_BOUNDS);
+        loc = nown + (lo - pf[p]);
+    }
+    if (loc > 65535) atomicOr(err, DEV_ERR_BOUNDS);
+    lconn[(int64_t)l * E + ne] = (uint16_t)loc;
+}
+
+__global__ void k_local_sizes(const int32_t* po, const int32_t* pf, int P, int* out) {
+    int m = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x)
+        m = max(m, (po[p + 1] - po[p]) + (pf[p + 1] - pf[p]));
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// Orders each patch's elements so that every aligned group of 32 has pairwise
+// node-disjoint elements where possible (greedy), making the shared-memory
+// accumulation of a warp conflict-free. One warp per patch; lane 0 decides.
+constexpr int kOrderWarps = 4;
+__global__ void __launch_bounds__(32 * kOrderWarps)
+k_patch_order(const uint16_t* __restrict__ lconn, int64_t E, const int32_t* __restrict__ pe, int P,
+              int32_t* __restrict__ wperm) {
+    __shared__ uint16_t sl[kOrderWarps][10][kPatchElems];
+    __shared__ uint32_t used[kOrderWarps][10 * kPatchElems / 32];
+    __shared__ uint8_t taken[kOrderWarps][kPatchElems];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = blockIdx.x * kOrderWarps + w;
+    if (p >= P) return;
+    const int e0 = pe[p], n_el = pe[p + 1] - e0;
+    for (int t = lane; t < 10 * n_el; t += 32) sl[w][t / n_el][t % n_el] = lconn[(int64_t)(t / n_el) * E + e0 + t % n_el];
+    for (int j = lane; j < n_el; j += 32) taken[w][j] = 0;
+    __syncwarp();
+    if (lane == 0) {
+        int nloc = 0;
+        for (int j = 0; j < n_el; ++j)
+            for (int l = 0; l < 10; ++l) nloc = max(nloc, (int)sl[w][l][j] + 1);
+        const int words = (nloc + 31) / 32;
+        int out = 0;
+        while (out < n_el) {
+            for (int k = 0; k < words; ++k) used[w][k] = 0u;
+            int cnt = 0;
+            for (int j = 0; j < n_el && cnt < 32; ++j) {
+                if (taken[w][j]) continue;
+                bool ok = true;
+                for (int l = 0; l < 10 && ok; ++l) {
+                    const int u = sl[w][l][j];
+                    ok = !((used[w][u >> 5] >> (u & 31)) & 1u);
+                }
+                if (!ok) continue;
+                for (int l = 0; l < 10; ++l) {
+                    const int u = sl[w][l][j];
+                    used[w][u >> 5] |= 1u << (u & 31);
+                }
+                taken[w][j] = 1;
+                wperm[e0 + out++] = e0 + j;
+                ++cnt;
+            }
+            // keep groups aligned with warps: top up with the next untaken elements
+            for (int j = 0; j < n_el && cnt < 32 && out < n_el; ++j) {
+                if (taken[w][j]) continue;
+                taken[w][j] = 1;
+                wperm[e0 + out++] = e0 + j;
+                ++cnt;
+            }
+        }
+    }
+}
+
+// Applies the within-patch order: eperm2[ne] = eperm[wperm[ne]] and the
+// patch-major paired connectivity (see PatchLayout::lc).
+__global__ void k_apply_order(const int32_t* __restrict__ wperm, const int32_t* __restrict__ eperm,
+                              const uint16_t* __restrict__ lconn, int64_t E, int P, int32_t* __restrict__ eperm2,
+                              uint32_t* __restrict__ lc) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)P * kPatchElems) return;
+    const int64_t p = t / kPatchElems, j = t % kPatchElems;
+    const int64_t ne = t;
+    if (ne < E) {
+        const int64_t src = wperm[ne];
+        eperm2[ne] = eperm[src];
+        for (int l2 = 0; l2 < 5; ++l2)
+            lc[(p * 5 + l2) * kPatchElems + j] =
+                (uint32_t)lconn[(int64_t)(2 * l2) * E + src] | (uint32_t)lconn[(int64_t)(2 * l2 + 1) * E + src] << 16;
+    } else {
+        for (int l2 = 0; l2 < 5; ++l2) lc[(p * 5 + l2) * kPatchElems + j] = 0u;
+    }
+}
+
+template <class F>
+void cub_call(cudaStream_t s, F&& f) {
+    size_t bytes = 0;
+    GEO_CUDA(f((void*)nullptr, bytes));
+    DevBuf<unsigned char> tmp(bytes + 16);
+    GEO_CUDA(f((void*)tmp.p, bytes));
+    GEO_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+
+void build_patches(cudaStream_t s, int64_t N, const double* xyz, int64_t E, const int32_t* conn, PatchLayout& L) {
+    L.n_elem = E;
+    L.n_nodes = N;
+    const int P = (int)cdiv(E, kPatchElems);
+    L.n_patches = P;
+    // ---- element order: Morton code of the vertex centroid
+    DevBuf<unsigned long long> bb(6);
+    DevBuf<double> lohi(6);
+    {
+        const unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
+        GEO_CUDA(cudaMemcpyAsync(bb.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+        k_bbox<<<std::min<unsigned>(nb(N), 2048), 256, 0, s>>>(xyz, N, bb.p);
+        k_bbox_decode<<<1, 32, 0, s>>>(bb.p, lohi.p);
+    }
+    {
+        DevBuf<uint64_t> k0(E), k1(E);
+        DevBuf<int32_t> i0(E);
+        L.eperm.alloc(E);
+        k_morton<<<nb(E), 256, 0, s>>>(xyz, conn, N, E, lohi.p, k0.p, i0.p);
+        cub_call(s, [&](void* t, size_t& b) {
+            return cub::DeviceRadixSort::SortPairs(t, b, k0.p, k1.p, i0.p, L.eperm.p, E, 0, 63, s);
+        });
+    }
+    // ---- node order: first touch over (patch-ordered element, local node)
+    L.nperm.alloc(N);
+    L.ninv.alloc(N);
+    DevBuf<int32_t> ft(N), ft_sorted(N);
+    {
+        DevBuf<int32_t> ids(N);
+        k_fill_max<<<nb(N), 256, 0, s>>>(ft.p, N);
+        k_first_touch<<<nb(E * 10), 256, 0, s>>>(conn, L.eperm.p, E, ft.p);
+        k_iota<<<nb(N), 256, 0, s>>>(ids.p, N);
+        cub_call(s, [&](void* t, size_t& b) {
+            return cub::DeviceRadixSort::SortPairs(t, b, ft.p, ft_sorted.p, ids.p, L.nperm.p, N, 0, 32, s);
+        });
+        int32_t last = 0;
+        GEO_CUDA(cudaMemcpy(&last, ft_sorted.p + N - 1, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        if (last >= (int32_t)(E * 10)) fail(GEO_ERR_UNSUPPORTED, "mesh has nodes that no element references");
+        k_inverse<<<nb(N), 256, 0, s>>>(L.nperm.p, N, L.ninv.p);
+    }
+    L.patch_elem.alloc(P + 1);
+    L.patch_own.alloc(P + 1);
+    k_patch_bounds<<<nb(P + 1), 256, 0, s>>>(ft_sorted.p, N, E, P, L.patch_elem.p, L.patch_own.p);
+    // ---- foreign lists
+    L.patch_foreign.alloc(P + 1);
+    L.shared.alloc(N);
+    GEO_CUDA(cudaMemsetAsync(L.shared.p, 0, N, s));
+    int64_t nf = 0;
+    {
+        DevBuf<uint64_t> k0(E * 10), k1(E * 10);
+        k_foreign_keys<<<nb(E * 10), 256, 0, s>>>(conn, L.eperm.p, L.ninv.p, L.patch_own.p, E, k0.p);
+        cub_call(s, [&](void* t, size_t& b) {
+            return cub::DeviceRadixSort::SortKeys(t, b, k0.p, k1.p, E * 10, 0, 64, s);
+        });
+        DevBuf<int64_t> nsel(1);
+        cub_call(s, [&](void* t, size_t& b) {
+            return cub::DeviceSelect::Unique(t, b, k1.p, k0.p, nsel.p, E * 10, s);
+        });
+        GEO_CUDA(cudaMemcpy(&nf, nsel.p, sizeof(int64_t), cudaMemcpyDeviceToHost));
+        uint64_t lastk = 0;
+        if (nf > 0) GEO_CUDA(cudaMemcpy(&lastk, k0.p + nf - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        if (nf > 0 && lastk == ~0ull) --nf;
+        L.foreign.alloc(std::max<int64_t>(nf, 1));
+        k_foreign_bounds<<<nb(P + 1), 256, 0, s>>>(k0.p, nf, P, L.patch_foreign.p);
+        if (nf > 0) k_foreign_nodes<<<nb(nf), 256, 0, s>>>(k0.p, nf, L.foreign.p, L.shared.p);
+        GEO_CUDA(cudaStreamSynchronize(s));
+    }
+    // ---- local connectivity and patch-table size
+    DevBuf<int> err(2);
+    GEO_CUDA(cudaMemsetAsync(err.p, 0, 2 * sizeof(int), s));
+    DevBuf<uint16_t> lconn(E * 10);
+    k_local_conn<<<nb(E * 10), 256, 0, s>>>(conn, L.eperm.p, L.ninv.p, L.patch_own.p, L.patch_foreign.p,
+                                           L.foreign.p, E, lconn.p, err.p);
+    k_local_sizes<<<std::min<unsigned>(nb(P), 1024), 256, 0, s>>>(L.patch_own.p, L.patch_foreign.p, P, err.p + 1);
+    GEO_CUDA(cudaGetLastError());
+    int h[2] = {0, 0};
+    GEO_CUDA(cudaMemcpyAsync(h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    GEO_CUDA(cudaStreamSynchronize(s));
+    if (h[0]) fail(GEO_ERR_UNSUPPORTED, "patch-local index out of range while building the element patches");
+    L.max_local = h[1];
+    // ---- conflict-avoiding element order inside each patch, patch-major connectivity
+    {
+        DevBuf<int32_t> wperm(E), eperm2(E);
+        k_patch_order<<<(unsigned)cdiv(P, kOrderWarps), 32 * kOrderWarps, 0, s>>>(lconn.p, E, L.patch_elem.p, P,
+                                                                                  wperm.p);
+        L.lc.alloc((size_t)P * 5 * kPatchElems);
+        k_apply_order<<<nb((int64_t)P * kPatchElems), 256, 0, s>>>(wperm.p, L.eperm.p, lconn.p, E, P, eperm2.p,
+                                                                    L.lc.p);
+        GEO_CUDA(cudaGetLastError());
+        GEO_CUDA(cudaStreamSynchronize(s));
+        L.eperm = std::move(eperm2);
+    }
+}
+
+}  // namespace geo

@@ -1,42 +1,48 @@
-// Element-patch layout of the matrix-free operator (host-built).
+// Element-patch layout of the matrix-free operator (built on the GPU).
 //
 // Elements are ordered along a Morton curve of their vertex centroids and cut
-// into patches of at most kPatchElems elements touching at most kPatchNodes
-// distinct nodes. Nodes are renumbered in first-touch order over that element
-// order, so each patch "owns" one contiguous range of new node ids (the nodes it
-// touches first); the other nodes it touches ("foreign") were owned by earlier
-// patches and are listed explicitly. Connectivity is stored as 16-bit indices
-// into the patch-local node table [own range | foreign list].
+// into patches of kPatchElems consecutive elements. Nodes are renumbered in
+// first-touch order over that element order, so each patch "owns" one
+// contiguous range of new node ids (the nodes it touches first); the other
+// nodes it touches ("foreign") were owned by earlier patches and are listed
+// explicitly. Connectivity is stored as 16-bit indices into the patch-local
+// node table [own range | foreign list].
 #pragma once
 
 #include <cstdint>
-#include <vector>
+
+#include "common.cuh"
 
 namespace geo {
 
 constexpr int kPatchElems = 384;
-constexpr int kPatchNodes = 1024;
 
-// node flag bits (new numbering)
-constexpr uint8_t kFlagDir0 = 1;    // component c Dirichlet: kFlagDir0 << c
+// node flag bits (patch numbering)
+constexpr uint8_t kFlagDir0 = 1;      // component c is Dirichlet: kFlagDir0 << c
 constexpr uint8_t kFlagShared = 128;  // touched by more than one patch
 
 struct PatchLayout {
     int64_t n_elem = 0, n_nodes = 0;
-    int64_t n_patches = 0;
-    int max_local = 0;                   // largest patch-local node table
-    std::vector<int32_t> eperm;          // new element -> original element
-    std::vector<int32_t> nperm;          // new node -> original node
-    std::vector<int32_t> ninv;           // original node -> new node
-    std::vector<int32_t> patch_elem;     // [n_patches + 1]
-    std::vector<int32_t> patch_own;      // [n_patches + 1] new node ids
-    std::vector<int32_t> patch_foreign;  // [n_patches + 1] offsets into foreign
-    std::vector<int32_t> foreign;        // new node ids, ascending per patch
-    std::vector<uint16_t> lconn;         // SoA [10][n_elem] patch-local indices
-    std::vector<uint8_t> shared;         // [n_nodes] new ids: 1 if shared
+    int n_patches = 0;
+    int max_local = 0;          // largest patch-local node table
+    DevBuf<int32_t> eperm;      // new element -> original element
+    DevBuf<int32_t> nperm;      // new node -> original node
+    DevBuf<int32_t> ninv;       // original node -> new node
+    DevBuf<int32_t> patch_elem;     // [n_patches + 1]
+    DevBuf<int32_t> patch_own;      // [n_patches + 1] new node ids
+    DevBuf<int32_t> patch_foreign;  // [n_patches + 1] offsets into foreign
+    DevBuf<int32_t> foreign;        // new node ids, ascending per patch
+    // Patch-major local connectivity, two 16-bit indices per word:
+    // lc[(p * 5 + l / 2) * kPatchElems + j] holds, in bits 16*(l%2).., the
+    // patch-local node index of local node l of the patch's element j (entries
+    // past a short last patch are 0). Within a patch, elements are ordered so that
+    // every aligned group of 32 (one warp) shares no node where possible.
+    DevBuf<uint32_t> lc;            // [n_patches][5][kPatchElems]
+    DevBuf<uint8_t> shared;         // [n_nodes] patch numbering: 1 if shared
 };
 
-// conn: AoS [E][10] original ids; xyz AoS [N][3].
-void build_patches(int64_t n_nodes, const double* xyz, int64_t n_elem, const int32_t* conn, PatchLayout& out);
+// xyz: device SoA [3][N]; conn: device SoA [10][E] (original numbering).
+void build_patches(cudaStream_t s, int64_t n_nodes, const double* xyz, int64_t n_elem, const int32_t* conn,
+                   PatchLayout& out);
 
 }  // namespace geo

@@ -77,6 +77,12 @@ class Context:
     def check(self, code, allow=()):
         return N.check(code, self.h, allow)
 
+    def stream_handle(self) -> int:
+        """cudaStream_t of this context (for torch.cuda.ExternalStream)."""
+        v = C.c_void_p()
+        self.check(N.lib().geo_ctx_stream(self.h, C.byref(v)))
+        return v.value or 0
+
     def sm_count(self) -> int:
         v = C.c_int()
         self.check(N.lib().geo_sm_count(self.h, C.byref(v)))

@@ -82,7 +82,8 @@ typedef struct geo_solver_stats {
     int32_t status;                 /* GEO_* code of the solve                      */
     int64_t fp64_residual_updates;  /* MIXED: number of FP64 residual refreshes     */
     double b_norm;
-    double kernel_time;             /* seconds inside the persistent PCG kernel     */
+    double kernel_time;             /* seconds of device work of the solve (CUDA events) */
+    int64_t kernel_launches;        /* kernels the solve launched                   */
 } geo_solver_stats;
 
 /* ------------------------------------------------------------------ context */
@@ -92,6 +93,9 @@ int geo_ctx_destroy(geo_ctx* ctx);
 const char* geo_last_error(const geo_ctx* ctx);
 const char* geo_version(void);
 int geo_sm_count(const geo_ctx* ctx, int* sm_count);
+/* The context's CUDA stream (cudaStream_t), so callers can order or time their
+ * own work against the library's launches. */
+int geo_ctx_stream(const geo_ctx* ctx, void** stream);
 
 /* ------------------------------------------------------------------ mesh */
 /* ImprovedMeshGenerator::generate_cube, mesh_generator_improved.rs:19-169 (host

@@ -534,6 +534,69 @@ orc_csr* orc_assemble_thermal_stiffness(int64_t n_nodes, const double* xyz, int6
     return triplets_to_csr(n_nodes, n_nodes, r, c, v);
 }
 
+// Same CSR as orc_assemble_thermal_stiffness (sorted columns, duplicates summed
+// in element order, structural zeros kept), built row by row under OpenMP
+// through a node -> (element, local) map instead of a global triplet sort, so
+// that the 128^3 system fits the host's memory and minutes. Used to prepare the
+// CPU baseline's input; the arithmetic of every K_e is the reference's.
+orc_csr* orc_assemble_thermal_stiffness_rows(int64_t n_nodes, const double* xyz, int64_t n_elem,
+                                             const int64_t* conn, const double* k_e, double k) {
+    std::vector<double> Ke((size_t)n_elem * 100);
+    int ok = 1;
+#pragma omp parallel for schedule(static) reduction(&& : ok)
+    for (int64_t e = 0; e < n_elem; ++e) {
+        double nodes[30];
+        gather_nodes(xyz, conn, e, nodes);
+        ok = ok && thermal_stiffness(nodes, k_e ? k_e[e] : k, &Ke[(size_t)e * 100]);
+    }
+    if (!ok) return nullptr;
+    std::vector<int64_t> ptr(n_nodes + 1, 0);
+    for (int64_t t = 0; t < n_elem * 10; ++t) ptr[conn[t] + 1]++;
+    for (int64_t i = 0; i < n_nodes; ++i) ptr[i + 1] += ptr[i];
+    std::vector<int64_t> inc(n_elem * 10);
+    {
+        std::vector<int64_t> cur(ptr.begin(), ptr.end() - 1);
+        for (int64_t t = 0; t < n_elem * 10; ++t) inc[cur[conn[t]]++] = t;  // element order
+    }
+    orc_csr* A = new orc_csr;
+    A->rows = A->cols = n_nodes;
+    A->indptr.assign(n_nodes + 1, 0);
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t i = 0; i < n_nodes; ++i) {
+        std::vector<int64_t> cols;
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+            const int64_t e = inc[p] / 10;
+            for (int j = 0; j < 10; ++j) cols.push_back(conn[10 * e + j]);
+        }
+        std::sort(cols.begin(), cols.end());
+        A->indptr[i + 1] = std::unique(cols.begin(), cols.end()) - cols.begin();
+    }
+    for (int64_t i = 0; i < n_nodes; ++i) A->indptr[i + 1] += A->indptr[i];
+    A->indices.resize(A->indptr[n_nodes]);
+    A->data.assign(A->indptr[n_nodes], 0.0);
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t i = 0; i < n_nodes; ++i) {
+        std::vector<int64_t> cols;
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+            const int64_t e = inc[p] / 10;
+            for (int j = 0; j < 10; ++j) cols.push_back(conn[10 * e + j]);
+        }
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        const int64_t b = A->indptr[i];
+        std::copy(cols.begin(), cols.end(), A->indices.begin() + b);
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+            const int64_t e = inc[p] / 10, l = inc[p] % 10;
+            for (int j = 0; j < 10; ++j) {
+                const int64_t c = conn[10 * e + j];
+                const int64_t pos = std::lower_bound(cols.begin(), cols.end(), c) - cols.begin();
+                A->data[b + pos] += Ke[(size_t)e * 100 + 10 * l + j];
+            }
+        }
+    }
+    return A;
+}
+
 // assembly.rs:130-154 (serial element loop)
 void orc_assemble_thermal_load(int64_t n_nodes, const double* xyz, int64_t n_elem,
                                const int64_t* conn, double Q, double* f) {
@@ -644,11 +707,74 @@ orc_csr* orc_apply_dirichlet_bcs(const orc_csr* K, const double* f, const uint8_
     return triplets_to_csr(n, K->cols, r, c, v);
 }
 
+// assembly.rs:168-230 with the same results as orc_apply_dirichlet_bcs (each
+// (row, col) occurs once, so the triplet merge is a per-row copy), row-parallel.
+orc_csr* orc_apply_dirichlet_bcs_rows(const orc_csr* K, const double* f, const uint8_t* mask, const double* g,
+                                      double* f_out) {
+    const int64_t n = K->rows;
+    const double cd = orc_char_diag(K);
+    orc_csr* B = new orc_csr;
+    B->rows = n;
+    B->cols = K->cols;
+    B->indptr.assign(n + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        if (mask[i]) {
+            B->indptr[i + 1] = 1;
+            f_out[i] = g[i] * cd;
+            continue;
+        }
+        double s = f[i];
+        int64_t c = 0;
+        for (int64_t p = K->indptr[i]; p < K->indptr[i + 1]; ++p) {
+            const int64_t j = K->indices[p];
+            if (mask[j]) s -= K->data[p] * g[j];
+            else ++c;
+        }
+        f_out[i] = s;
+        B->indptr[i + 1] = c;
+    }
+    for (int64_t i = 0; i < n; ++i) B->indptr[i + 1] += B->indptr[i];
+    B->indices.resize(B->indptr[n]);
+    B->data.resize(B->indptr[n]);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t o = B->indptr[i];
+        if (mask[i]) {
+            B->indices[o] = i;
+            B->data[o] = cd;
+            continue;
+        }
+        for (int64_t p = K->indptr[i]; p < K->indptr[i + 1]; ++p) {
+            const int64_t j = K->indices[p];
+            if (!mask[j]) {
+                B->indices[o] = j;
+                B->data[o] = K->data[p];
+                ++o;
+            }
+        }
+    }
+    return B;
+}
+
 orc_csr* orc_csr_from_triplets(int64_t n_rows, int64_t n_cols, int64_t n_trip, const int64_t* rows,
                                const int64_t* cols, const double* vals) {
     std::vector<int64_t> r(rows, rows + n_trip), c(cols, cols + n_trip);
     std::vector<double> v(vals, vals + n_trip);
     return triplets_to_csr(n_rows, n_cols, r, c, v);
+}
+// Copies an existing CSR (already sorted and merged) into an oracle handle.
+orc_csr* orc_csr_wrap(int64_t n_rows, int64_t n_cols, const int64_t* indptr, const int32_t* indices,
+                      const double* data) {
+    orc_csr* A = new orc_csr;
+    A->rows = n_rows;
+    A->cols = n_cols;
+    const int64_t nnz = indptr[n_rows];
+    A->indptr.assign(indptr, indptr + n_rows + 1);
+    A->indices.resize(nnz);
+    for (int64_t p = 0; p < nnz; ++p) A->indices[p] = indices[p];
+    A->data.assign(data, data + nnz);
+    return A;
 }
 int64_t orc_csr_rows(const orc_csr* A) { return A->rows; }
 int64_t orc_csr_nnz(const orc_csr* A) { return (int64_t)A->indices.size(); }

@@ -66,6 +66,9 @@ int orc_gravity_load(const double nodes[30], double rho, const double g[3], doub
 orc_csr* orc_assemble_thermal_stiffness(int64_t n_nodes, const double* xyz, int64_t n_elem,
                                         const int64_t* conn, const double* k_e, double k,
                                         int parallel);
+/* Same CSR, assembled row-parallel (OpenMP) through a node -> element map. */
+orc_csr* orc_assemble_thermal_stiffness_rows(int64_t n_nodes, const double* xyz, int64_t n_elem,
+                                             const int64_t* conn, const double* k_e, double k);
 void orc_assemble_thermal_load(int64_t n_nodes, const double* xyz, int64_t n_elem,
                                const int64_t* conn, double Q, double* f);
 orc_csr* orc_assemble_elasticity_stiffness(int64_t n_nodes, const double* xyz, int64_t n_elem,
@@ -77,10 +80,15 @@ void orc_assemble_gravity_load(int64_t n_nodes, const double* xyz, int64_t n_ele
 orc_csr* orc_apply_dirichlet_bcs(const orc_csr* K, const double* f, const uint8_t* dirichlet_mask,
                                  const double* dirichlet_values, double* f_out);
 double orc_char_diag(const orc_csr* K);
+/* Same result as orc_apply_dirichlet_bcs, row-parallel. */
+orc_csr* orc_apply_dirichlet_bcs_rows(const orc_csr* K, const double* f, const uint8_t* dirichlet_mask,
+                                      const double* dirichlet_values, double* f_out);
 
 /* ---- sparse matrices (sprs TriMat::to_csr semantics) ---- */
 orc_csr* orc_csr_from_triplets(int64_t n_rows, int64_t n_cols, int64_t n_trip, const int64_t* rows,
                                const int64_t* cols, const double* vals);
+orc_csr* orc_csr_wrap(int64_t n_rows, int64_t n_cols, const int64_t* indptr, const int32_t* indices,
+                      const double* data);
 int64_t orc_csr_rows(const orc_csr* A);
 int64_t orc_csr_nnz(const orc_csr* A);
 void orc_csr_copy(const orc_csr* A, int64_t* indptr, int64_t* indices, double* data);

@@ -74,6 +74,8 @@ def _declare(L):
         "orc_elasticity_stiffness": (C.c_int, [_D, C.c_double, C.c_double, _D]),
         "orc_gravity_load": (C.c_int, [_D, C.c_double, _D, _D]),
         "orc_assemble_thermal_stiffness": (_P, [C.c_int64, _D, C.c_int64, _I64, _D, C.c_double, C.c_int]),
+        "orc_assemble_thermal_stiffness_rows": (_P, [C.c_int64, _D, C.c_int64, _I64, _D, C.c_double]),
+        "orc_apply_dirichlet_bcs_rows": (_P, [_P, _D, _U8, _D, _D]),
         "orc_assemble_thermal_load": (None, [C.c_int64, _D, C.c_int64, _I64, C.c_double, _D]),
         "orc_assemble_elasticity_stiffness": (_P, [C.c_int64, _D, C.c_int64, _I64, _D, C.c_double,
                                                    C.c_double, C.c_int]),
@@ -81,6 +83,7 @@ def _declare(L):
         "orc_apply_dirichlet_bcs": (_P, [_P, _D, _U8, _D, _D]),
         "orc_char_diag": (C.c_double, [_P]),
         "orc_csr_from_triplets": (_P, [C.c_int64, C.c_int64, C.c_int64, _I64, _I64, _D]),
+        "orc_csr_wrap": (_P, [C.c_int64, C.c_int64, _I64, C.c_void_p, _D]),
         "orc_csr_rows": (C.c_int64, [_P]),
         "orc_csr_nnz": (C.c_int64, [_P]),
         "orc_csr_copy": (None, [_P, _I64, _I64, _D]),
@@ -319,6 +322,63 @@ def csr_apply(K: Csr, x):
     lib().orc_csr_apply(h, _d(_f64(x)), _d(y))
     lib().orc_csr_free(h)
     return y
+
+
+class ThermalSystem:
+    """K_bc and f_bc of the thermal problem held on the oracle side (no copies to numpy):
+    the row-parallel assembler + Dirichlet pass, then the reference CG on it."""
+
+    def __init__(self, xyz, conn, k_e, Q, mask, values):
+        L = lib()
+        xyz, conn = _f64(xyz), _i64(conn)
+        self.n = xyz.shape[0]
+        hk = L.orc_assemble_thermal_stiffness_rows(self.n, _d(xyz), conn.shape[0], _i(conn), _d(_f64(k_e)), 0.0)
+        f = np.empty(self.n)
+        L.orc_assemble_thermal_load(self.n, _d(xyz), conn.shape[0], _i(conn), Q, _d(f))
+        mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        self.fb = np.empty(self.n)
+        self.h = L.orc_apply_dirichlet_bcs_rows(hk, _d(f), mask.ctypes.data_as(_U8), _d(_f64(values)),
+                                                _d(self.fb))
+        L.orc_csr_free(hk)
+        self.nnz = L.orc_csr_nnz(self.h)
+
+    def cg(self, max_iterations, tolerance=1e-8, abs_tolerance=1e-12):
+        x = np.empty(self.n)
+        st = OrcStats()
+        lib().orc_cg_solve(self.h, _d(self.fb), int(max_iterations), tolerance, abs_tolerance, 1, _d(x),
+                           C.byref(st))
+        return x, st
+
+    def __del__(self):
+        try:
+            lib().orc_csr_free(self.h)
+        except Exception:
+            pass
+
+
+class CsrHandle:
+    """Oracle-side copy of a CSR given as (int64 indptr, int32 indices, float64 data)."""
+
+    def __init__(self, n_rows, n_cols, indptr, indices, data):
+        indptr = np.ascontiguousarray(indptr, np.int64)
+        indices = np.ascontiguousarray(indices, np.int32)
+        data = np.ascontiguousarray(data, np.float64)
+        self.n_rows = n_rows
+        self.h = lib().orc_csr_wrap(n_rows, n_cols, _i(indptr), indices.ctypes.data, _d(data))
+
+    def cg(self, b, max_iterations, tolerance=1e-8, abs_tolerance=1e-12, use_preconditioner=True):
+        """The reference loop (iterative.rs:46-119) on this matrix."""
+        x = np.empty(self.n_rows)
+        st = OrcStats()
+        lib().orc_cg_solve(self.h, _d(_f64(b)), int(max_iterations), tolerance, abs_tolerance,
+                           int(bool(use_preconditioner)), _d(x), C.byref(st))
+        return x, st
+
+    def __del__(self):
+        try:
+            lib().orc_csr_free(self.h)
+        except Exception:
+            pass
 
 
 # ------------------------------------------------------------------- solvers
