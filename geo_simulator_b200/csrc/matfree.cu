@@ -30,6 +30,11 @@ __global__ void k_lift_finish(const uint8_t* flags, int dpn, int64_t n, double c
     }
 }
 
+__global__ void k_scale(double* v, int64_t n, double a) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] *= a;
+}
+
 template <class T>
 __global__ void k_zero_dir(const uint8_t* flags, int dpn, int64_t n, T* v) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -211,6 +216,15 @@ __global__ void k_gather_diag(const int32_t* ptr, const int32_t* inc, const doub
         s += ediag[(int64_t)(el / 10) * 10 * dpn + dpn * (el % 10) + c];
     }
     diag[t] = s;
+}
+
+// max_i |v_i w_i| as the bit pattern of a non-negative double
+__global__ void k_max_abs_scaled(const double* v, const double* w, int64_t n, unsigned long long* out) {
+    double m = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(v[i] * w[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
 __global__ void k_max_abs(const double* v, int64_t n, unsigned long long* out) {
@@ -924,7 +938,27 @@ int geo_vjp(geo_op* op, const double* f, const double* u, const double* dJ_du, c
     to_new(op, dg, op->bvec.p);
     k_zero_dir<double><<<nblk(n), 256, 0, s>>>(op->flags.p, op->dpn, n, op->bvec.p);
     check_launch(op->ctx, "adjoint rhs");
-    const int status = solve_new(op, o, st);
+    // The adjoint system is linear in its right-hand side: solve with dJ/du scaled
+    // so that its Jacobi-preconditioned form D^-1 b has unit max-norm (lambda is
+    // then O(1)) and scale lambda back, so that the absolute breakdown and
+    // stopping thresholds of the CG loop do not depend on the misfit's units or
+    // on the stiffness scale.
+    DevBuf<unsigned long long> mx(1);
+    GEO_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(unsigned long long), s));
+    k_max_abs_scaled<<<nblk(n), 256, 0, s>>>(op->bvec.p, op->dinv64.p, n, mx.p);
+    unsigned long long bits = 0;
+    GEO_CUDA(cudaMemcpyAsync(&bits, mx.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    sync(op->ctx, "adjoint scale");
+    double zmax;
+    std::memcpy(&zmax, &bits, sizeof(double));
+    int status = GEO_OK;
+    if (zmax > 0.0) {
+        k_scale<<<nblk(n), 256, 0, s>>>(op->bvec.p, n, 1.0 / zmax);  // b / zmax
+        status = solve_new(op, o, st);
+        k_scale<<<nblk(n), 256, 0, s>>>(op->xvec.p, n, zmax);        // lambda = zmax * lambda_scaled
+    } else {
+        GEO_CUDA(cudaMemsetAsync(op->xvec.p, 0, n * sizeof(double), s));
+    }
     to_orig(op, op->xvec.p, lo.p);
     const geo_mesh* m = op->mesh;
     k_elem_gradient<<<(unsigned)cdiv(op->E, 128), 128, 0, s>>>(op->phys, m->xyz.p, m->conn.p, op->N, op->E,
