@@ -97,6 +97,7 @@ _SIGS = {
     "geo_op_apply": [_P, _DP, _DP, _I32],
     "geo_op_lift_rhs": [_P, _DP, _DP],
     "geo_op_diagonal": [_P, _DP],
+    "geo_cg_solve_noalloc": [_P, _P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_cg_solve_matfree": [_P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_op_element_gradient": [_P, _DP, _DP, _DP],
     "geo_forward": [_P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],

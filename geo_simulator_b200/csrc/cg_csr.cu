@@ -6,6 +6,8 @@
 // Jacobi scaling, axpys, and dot products reduced by warp shuffles into
 // per-block partials that every block sums in the same fixed order after a
 // bounded grid barrier (so all blocks take identical, deterministic decisions).
+#include <mutex>
+
 #include "pcg_common.cuh"
 
 namespace geo {
@@ -221,3 +223,142 @@ int geo_cg_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_o
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of geo_cg_solve (no counterpart in the reference).
+//
+// Who needs it: callers that must not call cudaMalloc/cudaFree between solves --
+// a host loop whose device memory is fully reserved by another allocator (a
+// caching allocator that has already taken the free memory), or a latency loop
+// that cannot afford cudaFree's implicit device-wide synchronisation. It runs the
+// same k_csr_pcg kernel as geo_cg_solve, with the four work vectors, the block
+// partials, the barrier word and the result taken from one file-scope device
+// array instead of cudaMalloc, so results are bit-identical to geo_cg_solve.
+//
+// Limits and rules:
+//  * at most GEO_NOALLOC_MAX_ROWS rows and kNoAllocMaxBlocks persistent blocks;
+//    larger systems are rejected with GEO_ERR_INVALID_ARG;
+//  * b and x must be device memory on the context's device (no host staging);
+//  * the GridSync word and the PcgResult slot must start at zero: they are
+//    cleared with cudaMemsetAsync on the context stream before every launch
+//    (a timed-out barrier can leave the count non-zero);
+//  * one scratch array per device: two calls that overlap on the same device
+//    (different threads or contexts) race on it and must be serialised;
+//  * the first call on a device looks the array up with cudaGetSymbolAddress,
+//    which can make the runtime load this module and reserve the array; make
+//    that first call before the phase that must not allocate, and before any
+//    stream capture begins.
+namespace geo {
+namespace {
+
+constexpr int kNoAllocMaxBlocks = 4096;
+constexpr size_t kNoAllocVecBytes = (size_t)GEO_NOALLOC_MAX_ROWS * sizeof(double);
+constexpr size_t kNoAllocPartBytes = (size_t)kNoAllocMaxBlocks * 4 * sizeof(double);
+constexpr size_t kNoAllocOffPart = 4 * kNoAllocVecBytes;                    // r, p, q, dinv
+constexpr size_t kNoAllocOffSync = kNoAllocOffPart + 2 * kNoAllocPartBytes;  // part_a, part_b
+constexpr size_t kNoAllocOffRes = kNoAllocOffSync + 256;
+constexpr size_t kNoAllocBytes = kNoAllocOffRes + 256;
+static_assert(sizeof(GridSync) <= 256 && sizeof(PcgResult) <= 256, "scratch slots too small");
+static_assert(kNoAllocVecBytes % 256 == 0 && kNoAllocPartBytes % 256 == 0, "slots stay 256-byte aligned");
+
+// 8.25 MiB per device: 4 x 2 MiB vectors + 2 x 128 KiB partials + two 256 B slots.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (which must be current).
+unsigned char* noalloc_scratch(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices) fail(GEO_ERR_UNSUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            fail(GEO_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[device] = static_cast<unsigned char*>(p);
+    }
+    return g_noalloc_addr[device];
+}
+
+bool on_device(const void* p, int device) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == device;
+}
+
+}  // namespace
+}  // namespace geo
+
+extern "C" int geo_cg_solve_noalloc(geo_ctx* ctx, const geo_csr* A, const double* b_dev,
+                                    const geo_cg_opts* opts, double* x_dev, geo_solver_stats* stats) {
+    GEO_API_BEGIN(ctx)
+    GEO_CHECK_ARG(ctx && A, "NULL argument");
+    unsigned char* base = noalloc_scratch(ctx->device);  // first call: symbol lookup
+    GEO_CHECK_ARG(A->n_rows == A->n_cols, "matrix must be square");
+    const int64_t n = A->n_rows;
+    if (n > GEO_NOALLOC_MAX_ROWS)
+        fail(GEO_ERR_INVALID_ARG, "geo_cg_solve_noalloc: " + std::to_string(n) +
+                                      " rows exceed GEO_NOALLOC_MAX_ROWS (" +
+                                      std::to_string((long long)GEO_NOALLOC_MAX_ROWS) + "); use geo_cg_solve");
+    if (n > 0)
+        GEO_CHECK_ARG(b_dev && x_dev && on_device(b_dev, ctx->device) && on_device(x_dev, ctx->device),
+                      "geo_cg_solve_noalloc: b and x must be device memory on the context's device");
+    geo_cg_opts o;
+    cg_opts_fill(opts, o);
+    GEO_CHECK_ARG(o.max_iterations >= 0, "max_iterations must be >= 0");
+    const int nb = persistent_blocks(ctx, k_csr_pcg, kBS, 0);
+    if (nb > kNoAllocMaxBlocks) fail(GEO_ERR_UNSUPPORTED, "geo_cg_solve_noalloc: persistent grid too large");
+    cudaStream_t s = ctx->stream;
+    double* vec = reinterpret_cast<double*>(base);
+    GridSync* gs = reinterpret_cast<GridSync*>(base + kNoAllocOffSync);
+    PcgResult* res = reinterpret_cast<PcgResult*>(base + kNoAllocOffRes);
+    CsrPcgArgs args{};
+    args.indptr = A->indptr.p;
+    args.indices = A->indices.p;
+    args.data = A->data.p;
+    args.n = n;
+    args.b = b_dev;
+    args.x = x_dev;
+    args.r = vec;
+    args.p = vec + GEO_NOALLOC_MAX_ROWS;
+    args.q = vec + 2 * (size_t)GEO_NOALLOC_MAX_ROWS;
+    args.dinv = vec + 3 * (size_t)GEO_NOALLOC_MAX_ROWS;
+    args.part_a = reinterpret_cast<double*>(base + kNoAllocOffPart);
+    args.part_b = reinterpret_cast<double*>(base + kNoAllocOffPart + kNoAllocPartBytes);
+    args.gs = gs;
+    args.res = res;
+    args.timeout_ns = (unsigned long long)(o.timeout_seconds * 1e9);
+    args.max_it = o.max_iterations;
+    args.tol = o.tolerance;
+    args.abs_tol = o.abs_tolerance;
+    args.use_prec = o.use_preconditioner;
+    GEO_CUDA(cudaMemsetAsync(gs, 0, sizeof(GridSync), s));
+    GEO_CUDA(cudaMemsetAsync(res, 0, sizeof(PcgResult), s));
+    GEO_CUDA(cudaEventRecord(ctx->ev0, s));
+    launch_persistent(ctx, k_csr_pcg, kBS, 0, args, nb);
+    GEO_CUDA(cudaEventRecord(ctx->ev1, s));
+    PcgResult r{};
+    GridSync g{};
+    GEO_CUDA(cudaMemcpyAsync(&r, res, sizeof(r), cudaMemcpyDeviceToHost, s));
+    GEO_CUDA(cudaMemcpyAsync(&g, gs, sizeof(g), cudaMemcpyDeviceToHost, s));
+    sync(ctx, "geo_cg_solve_noalloc");
+    float ms = 0.f;
+    GEO_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (g.error & DEV_ERR_TIMEOUT) {
+        fill_stats(stats, r, ms * 1e-3, GEO_ERR_TIMEOUT);
+        fail(GEO_ERR_TIMEOUT, "PCG grid barrier timed out");
+    }
+    const int status = r.converged ? GEO_OK : (r.breakdown ? GEO_ERR_BREAKDOWN : GEO_NOT_CONVERGED);
+    fill_stats(stats, r, ms * 1e-3, status);
+    if (stats) stats->kernel_launches = 1;
+    if (status != GEO_OK) {
+        record_error(ctx, status, r.breakdown ? "CG breakdown: |p^T A p| < 1e-30" : "CG did not converge");
+        return status;
+    }
+    GEO_API_END
+}

@@ -181,6 +181,20 @@ void geo_cg_opts_default(geo_cg_opts* opts);
 int geo_cg_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_opts* opts,
                  double* x, geo_solver_stats* stats);
 
+/* No counterpart in the reference. geo_cg_solve without any device allocation, for
+ * callers that must not call cudaMalloc/cudaFree between solves (device memory
+ * held by another allocator; loops that cannot take cudaFree's device-wide sync).
+ * Same kernel and results as geo_cg_solve. Work vectors come from one static
+ * device array per device (8.25 MiB), so: n_rows <= GEO_NOALLOC_MAX_ROWS (else
+ * GEO_ERR_INVALID_ARG); b_dev and x_dev must be device memory on the context's
+ * device; calls that overlap on one device race on the array and must be
+ * serialised; the first call on a device looks the array up (the runtime may load
+ * the module then), so make it before the allocation-free phase and before any
+ * stream capture. The barrier word and result slot are zeroed before each launch. */
+#define GEO_NOALLOC_MAX_ROWS 262144
+int geo_cg_solve_noalloc(geo_ctx* ctx, const geo_csr* A, const double* b_dev, const geo_cg_opts* opts,
+                         double* x_dev, geo_solver_stats* stats);
+
 /* ------------------------------------------------------------------ K5/K6: matrix-free */
 /* Matrix-free Dirichlet-eliminated operator K_bc of the thermal problem (the
  * operator apply_dirichlet_bcs(assemble_thermal_stiffness_parallel(..)) builds,
