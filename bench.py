@@ -38,11 +38,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from geo_simulator_b200.kernel_timing import patch_pcg_bytes, update_bytes  # noqa: E402
+
 # Iterations of the FP64 Jacobi-PCG (the reference algorithm) to rel-res 1e-8 on the
 # n^3 log-normal-k system, measured on the GPU by this repository's FP64 solver
 # (same loop, same stopping rule). The reference arm times its per-iteration
 # cost on the host and scales by this count, so it never touches the GPU.
-FP64_ITERS = {}
+FP64_ITERS = {128: 1050}
 
 METRIC = "Tet10 PCG solve time @rel-res 1e-8: mixed vs FP64 GPU; adjoint/forward ratio"
 LX, LY, LZ = 1000.0, 1000.0, 600.0
@@ -79,9 +81,17 @@ def apply_bytes(E, N, s):
 
 
 def solve_bytes(E, N, iters, nupd):
-    """Algorithmic bytes of one mixed solve: per FP32 PCG iteration one FP32 apply
-    plus 8 FP32 vector streams; per FP64 refresh one FP64 apply plus 4 FP64 streams."""
-    return iters * (apply_bytes(E, N, 4) + 8 * N * 4) + nupd * (apply_bytes(E, N, 8) + 4 * N * 8)
+    """Algorithmic bytes of one mixed solve: per FP32 PCG iteration one patch-kernel
+    and one node-update launch; per FP64 refresh one FP64 apply plus 4 FP64 streams."""
+    return (iters * (patch_pcg_bytes(E, N, 4) + update_bytes(N, 4))
+            + nupd * (apply_bytes(E, N, 8) + 4 * N * 8))
+
+
+# DRAM bytes (read + write) per element of one FP32 PCG-mode patch-kernel launch,
+# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the 96^3 cube
+# (5,308,416 elements: 420.7 MB per launch); the traffic scales with the element
+# count (the node/element ratio of the cube is 1.35 at both sizes).
+PATCH_PCG_F32_DRAM_BYTES_PER_ELEMENT = 79.26
 
 
 class ClockSampler:
@@ -246,9 +256,19 @@ def run_ours(args, ws, rank, local, pg):
     if not args.quick and rank == 0:
         extras.update(adjoint_ratio(ctx, args))
 
+    # dominant kernel: the FP32 patch kernel in PCG mode, timed launch by launch with
+    # CUDA events on the context stream right after the timed region
+    kt_iters = 50
+    pms, ums = C.c_double(), C.c_double()
+    ctx.check(N.lib().geo_op_time_pcg_kernels(op.h, fb.data_ptr(), N.PRECISION_MIXED, kt_iters,
+                                              C.byref(pms), C.byref(ums)))
+    patch_s, update_s = pms.value / 1e3, ums.value / 1e3
     hbm, peak_kind = peaks()
+    pbytes = patch_pcg_bytes(E, Nn, 4)
+    ubytes = update_bytes(Nn, 4)
+    achieved = pbytes / patch_s / 1e9
+    traffic = (PATCH_PCG_F32_DRAM_BYTES_PER_ELEMENT * E) if PATCH_PCG_F32_DRAM_BYTES_PER_ELEMENT else None
     abytes = solve_bytes(E, Nn, iters, nupd)
-    achieved = abytes / kern / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -260,11 +280,18 @@ def run_ours(args, ws, rank, local, pg):
         "iterations": iters, "fp64_residual_updates": nupd,
         "dofs_per_s": Nn * ws / (t_mixed / args.steps),
         "pcg_iterations_per_s": iters / (t_mixed / args.steps),
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": int(sum(s_.kernel_launches for s_ in st_mixed)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "k_mf_pcg<ThermalK<double,1>,ThermalK<float,1>,true>",
-                     "kernel_s": kern, "algorithmic_bytes": abytes},
+                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_patch<ThermalK<float,1>, float, MODE_PCG, 2>",
+                     "algorithmic_bytes_per_launch": pbytes, "launch_s": patch_s,
+                     "timing": f"CUDA events between launches, {kt_iters} PCG iterations after the timed region",
+                     "node_update": {"kernel": "k_pcg_update<float, 1, true>", "launch_s": update_s,
+                                     "algorithmic_bytes_per_launch": ubytes,
+                                     "achieved": ubytes / update_s / 1e9,
+                                     "frac": ubytes / update_s / 1e9 / hbm},
+                     "solve": {"algorithmic_bytes": abytes, "device_s": kern,
+                               "achieved": abytes / kern / 1e9, "frac": abytes / kern / 1e9 / hbm}},
         "clocks": clk,
     }
     line.update(extras)

@@ -102,6 +102,7 @@ _SIGS = {
     "geo_op_element_gradient": [_P, _DP, _DP, _DP],
     "geo_forward": [_P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_vjp": [_P, _DP, _DP, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
+    "geo_op_time_pcg_kernels": [_P, _DP, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "geo_op_destroy": [_P],
     "geo_debug_barrier_timeout": [_P, _D],
 }

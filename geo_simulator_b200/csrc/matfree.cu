@@ -609,43 +609,35 @@ void enqueue_iteration(geo_op* op, cudaStream_t s, const PatchArgs<T>& pa, const
     k_pcg_update<T, K::DPN, MIXED><<<(unsigned)op->node_grid, kNodeBS, 0, s>>>(na);
 }
 
-// Jacobi-PCG on K_bc; b_new / x_new in patch numbering (device). Iterations run
-// in CUDA-graph chunks of kChunk (kernels turn into no-ops once the device state
-// says done or refresh); the host looks at the state between chunks and runs the
-// FP64 refresh of the mixed solver when it is requested.
-int solve_new(geo_op* op, const geo_cg_opts& o, geo_solver_stats* st) {
-    geo_ctx* ctx = op->ctx;
-    const double* b_new = op->bvec.p;
-    double* x_new = op->xvec.p;
-    cudaStream_t s = ctx->stream;
-    GEO_CHECK_ARG(o.use_preconditioner, "the matrix-free solver is Jacobi-preconditioned only");
-    const bool mixed = o.precision == GEO_PRECISION_MIXED;
-    const int64_t n = op->ndof;
-    // workspace: FP64 mode: r, q, p0, p1 (double); mixed: w64 (double) + xs, r, q, p0, p1 (float)
-    op->w64.ensure((size_t)(mixed ? 1 : 4) * n);
-    if (mixed) op->w32.ensure((size_t)5 * n);
-    PcgState init{};
-    init.tol = o.tolerance;
-    init.abs_tol = o.abs_tolerance;
-    init.delta = o.reliable_delta;
-    init.cd = op->cd;
-    init.max_it = o.max_iterations;
-    GEO_CUDA(cudaMemcpyAsync(op->state.p, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+// Kernel arguments of the PCG loop over the operator's workspace (FP64 mode: r, q,
+// p0, p1 in w64; mixed: w64 plus xs, r, q, p0, p1 in w32), allocated on first use.
+struct PcgLaunchArgs {
     NodeArgs<double> n64{};
     NodeArgs<float> n32{};
     PatchArgs<double> p64{};
     PatchArgs<float> p32{};
+};
+
+PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
+    const int64_t n = op->ndof;
+    op->w64.ensure((size_t)(mixed ? 1 : 4) * n);
+    if (mixed) op->w32.ensure((size_t)5 * n);
+    PcgLaunchArgs a;
+    NodeArgs<double>& n64 = a.n64;
+    NodeArgs<float>& n32 = a.n32;
+    PatchArgs<double>& p64 = a.p64;
+    PatchArgs<float>& p32 = a.p32;
     n64.flags = n32.flags = op->flags.p;
     n64.n = n32.n = n;
     n64.dpn = n32.dpn = op->dpn;
     n64.st = n32.st = p64.st = p32.st = op->state.p;
     p64.err = p32.err = &op->state.p->err;
     n64.part = n32.part = op->part.p;
-    p64.part = p32.part = op->part.p + op->node_grid * 0;  // patch and node kernels never overlap
-    n64.b = n32.b = b_new;
-    n64.x64 = n32.x64 = x_new;
+    p64.part = p32.part = op->part.p;  // patch and node kernels never overlap
+    n64.b = n32.b = op->bvec.p;
+    n64.x64 = n32.x64 = op->xvec.p;
     if (!mixed) {
-        n64.x = x_new;
+        n64.x = op->xvec.p;
         n64.r = op->w64.p;
         n64.q = op->w64.p + n;
         n64.pbuf0 = op->w64.p + 2 * n;
@@ -670,15 +662,47 @@ int solve_new(geo_op* op, const geo_cg_opts& o, geo_solver_stats* st) {
         p32.pbuf1 = n32.pbuf1;
         p32.y = n32.q;
     }
+    return a;
+}
+
+// Writes the initial PcgState and launches the start kernels (x = 0, r = b, ||b||).
+void pcg_start(geo_op* op, bool mixed, const PcgState& init, const PcgLaunchArgs& a) {
+    cudaStream_t s = op->ctx->stream;
+    GEO_CUDA(cudaMemcpyAsync(op->state.p, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const unsigned ng = (unsigned)op->node_grid;
+    if (mixed) {
+        k_mixed_init1<<<ng, kNodeBS, 0, s>>>(a.n32);
+        k_mixed_init2<<<ng, kNodeBS, 0, s>>>(a.n32);
+    } else {
+        k_pcg_init<double><<<ng, kNodeBS, 0, s>>>(a.n64);
+    }
+    check_launch(op->ctx, "pcg init");
+}
+
+// Jacobi-PCG on K_bc; b_new / x_new in patch numbering (device). Iterations run
+// in CUDA-graph chunks of kChunk (kernels turn into no-ops once the device state
+// says done or refresh); the host looks at the state between chunks and runs the
+// FP64 refresh of the mixed solver when it is requested.
+int solve_new(geo_op* op, const geo_cg_opts& o, geo_solver_stats* st) {
+    geo_ctx* ctx = op->ctx;
+    double* x_new = op->xvec.p;
+    cudaStream_t s = ctx->stream;
+    GEO_CHECK_ARG(o.use_preconditioner, "the matrix-free solver is Jacobi-preconditioned only");
+    const bool mixed = o.precision == GEO_PRECISION_MIXED;
+    PcgState init{};
+    init.tol = o.tolerance;
+    init.abs_tol = o.abs_tolerance;
+    init.delta = o.reliable_delta;
+    init.cd = op->cd;
+    init.max_it = o.max_iterations;
+    const PcgLaunchArgs la = pcg_args(op, mixed);
+    const NodeArgs<float>& n32 = la.n32;
+    const PatchArgs<double>& p64 = la.p64;
+    const PatchArgs<float>& p32 = la.p32;
+    const NodeArgs<double>& n64 = la.n64;
     const unsigned ng = (unsigned)op->node_grid;
     GEO_CUDA(cudaEventRecord(ctx->ev0, s));
-    if (mixed) {
-        k_mixed_init1<<<ng, kNodeBS, 0, s>>>(n32);
-        k_mixed_init2<<<ng, kNodeBS, 0, s>>>(n32);
-    } else {
-        k_pcg_init<double><<<ng, kNodeBS, 0, s>>>(n64);
-    }
-    check_launch(ctx, "pcg init");
+    pcg_start(op, mixed, init, la);
     // (re)build the chunk graph when the buffers it captured changed
     const int pi = mixed ? 1 : 0;
     const void* key0 = mixed ? (const void*)op->w32.p : (const void*)op->w64.p;
@@ -743,6 +767,58 @@ int solve_new(geo_op* op, const geo_cg_opts& o, geo_solver_stats* st) {
     fill_stats(st, r, ms * 1e-3, status);
     if (st) st->kernel_launches = launches;
     return status;
+}
+
+// Device time of the two kernels of one PCG iteration, launch by launch: `iters`
+// iterations from x = 0, r = op->bvec, with the stopping, refresh and
+// iteration-limit tests unable to fire (tolerances 0, delta 0, no limit), so every
+// launch does the full work of an iteration of a real solve. Events are
+// recorded on the context stream between the launches.
+void time_iterations(geo_op* op, bool mixed, int iters, double* patch_ms, double* update_ms) {
+    geo_ctx* ctx = op->ctx;
+    cudaStream_t s = ctx->stream;
+    PcgState init{};
+    init.cd = op->cd;
+    init.max_it = 1LL << 60;
+    const PcgLaunchArgs la = pcg_args(op, mixed);
+    pcg_start(op, mixed, init, la);
+    std::vector<cudaEvent_t> ev((size_t)2 * iters + 1, nullptr);
+    struct Guard {
+        std::vector<cudaEvent_t>& v;
+        ~Guard() {
+            for (auto e : v)
+                if (e) cudaEventDestroy(e);
+        }
+    } guard{ev};
+    for (auto& e : ev) GEO_CUDA(cudaEventCreate(&e));
+    const unsigned ng = (unsigned)op->node_grid;
+    with_kernels(op, [&](auto k64, auto k32) {
+        for (int i = 0; i < iters; ++i) {
+            GEO_CUDA(cudaEventRecord(ev[2 * i], s));
+            if (mixed) launch_patch<decltype(k32), float, MODE_PCG>(op, 1, s, op->qd32.p, la.p32);
+            else launch_patch<decltype(k64), double, MODE_PCG>(op, 0, s, op->qd64.p, la.p64);
+            GEO_CUDA(cudaEventRecord(ev[2 * i + 1], s));
+            if (mixed) k_pcg_update<float, decltype(k32)::DPN, true><<<ng, kNodeBS, 0, s>>>(la.n32);
+            else k_pcg_update<double, decltype(k64)::DPN, false><<<ng, kNodeBS, 0, s>>>(la.n64);
+        }
+    });
+    GEO_CUDA(cudaEventRecord(ev[2 * iters], s));
+    check_launch(ctx, "timed PCG iterations");
+    sync(ctx, "timed PCG iterations");
+    PcgState h{};
+    GEO_CUDA(cudaMemcpy(&h, op->state.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h.err) fail(GEO_ERR_TIMEOUT, "matrix-free PCG: a bounded device-side wait timed out");
+    if (h.flags & ST_DONE) fail(GEO_ERR_BREAKDOWN, "timed PCG iterations stopped early (breakdown)");
+    double tp = 0.0, tu = 0.0;
+    for (int i = 0; i < iters; ++i) {
+        float a = 0.f, b = 0.f;
+        GEO_CUDA(cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]));
+        GEO_CUDA(cudaEventElapsedTime(&b, ev[2 * i + 1], ev[2 * i + 2]));
+        tp += a;
+        tu += b;
+    }
+    *patch_ms = tp / iters;
+    *update_ms = tu / iters;
 }
 
 int finish_status(geo_ctx* ctx, int status) {
@@ -968,6 +1044,19 @@ int geo_vjp(geo_op* op, const double* f, const double* u, const double* dJ_du, c
     copy_out(dJ_dlncoef, ge.p, op->E, s);
     sync(op->ctx, "geo_vjp");
     return finish_status(op->ctx, status);
+    GEO_API_END
+}
+
+int geo_op_time_pcg_kernels(geo_op* op, const double* b, int32_t precision, int32_t iterations, double* patch_ms,
+                            double* update_ms) {
+    GEO_API_BEGIN(op ? op->ctx : nullptr)
+    GEO_CHECK_ARG(op && b && patch_ms && update_ms, "NULL argument");
+    GEO_CHECK_ARG(iterations >= 1 && iterations <= 4096, "iterations must be in [1, 4096]");
+    cudaStream_t s = op->ctx->stream;
+    DevBuf<double> tb;
+    const double* db = stage_in(b, op->ndof, tb, s);
+    to_new(op, db, op->bvec.p);
+    time_iterations(op, precision == GEO_PRECISION_MIXED, iterations, patch_ms, update_ms);
     GEO_API_END
 }
 

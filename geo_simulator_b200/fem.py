@@ -461,11 +461,13 @@ class SolverStats:
     status: int = 0
     fp64_residual_updates: int = 0
     b_norm: float = 0.0
+    kernel_launches: int = 0
 
     @classmethod
     def from_c(cls, s: N.SolverStatsC):
         return cls(int(s.iterations), float(s.residual_norm), float(s.relative_residual), bool(s.converged),
-                   float(s.solve_time), int(s.status), int(s.fp64_residual_updates), float(s.b_norm))
+                   float(s.solve_time), int(s.status), int(s.fp64_residual_updates), float(s.b_norm),
+                   int(s.kernel_launches))
 
 
 class ConjugateGradient:

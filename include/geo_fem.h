@@ -2,8 +2,8 @@
  * geo_fem.h -- C ABI of the B200 (sm_100a) Tet10 FEM hot path.
  *
  * Drop-in for the Rust hot path of msahamed/geo_simulator:
- *   src/fem/element.rs, src/fem/assembly.rs, src/mechanics/*, src/linalg/{solver,
- *   iterative,preconditioner}.rs.
+ *   src/fem/element.rs, src/fem/assembly.rs, the src/mechanics/ element, strain,
+ *   constitutive and body-force files, src/linalg/{solver,iterative,preconditioner}.rs.
  * Each entry point names the reference item it replaces (file:line inside the
  * reference project). A Rust crate binds these with `extern "C"`; the
  * Python host package (geo_simulator_b200) and include/geofem.hpp bind them too.
@@ -214,8 +214,11 @@ int geo_op_apply(geo_op* op, const double* x, double* y, int32_t precision);
 int geo_op_lift_rhs(geo_op* op, const double* f, double* f_bc);
 /* diag(K_bc), the Jacobi diagonal (preconditioner.rs:37-51). */
 int geo_op_diagonal(geo_op* op, double* diag);
-/* Jacobi-PCG on K_bc in one persistent kernel (matvec, Jacobi scaling, axpys and
- * grid-reduced dot products). FP64: the reference's stopping rule on the recursive
+/* Jacobi-PCG on K_bc, two kernels per iteration run from CUDA graphs of 16
+ * iterations: the patch kernel applies K_bc fused with p = D^-1 r + beta p and the
+ * p.Ap reduction; the node kernel does the axpys, r.r and r.z and the stopping
+ * test (single-pass grid reductions, scalars resident on the device, no host
+ * round trip inside a graph). FP64: the reference's stopping rule on the recursive
  * residual. MIXED: FP32 inner PCG with FP32 accumulation; the FP64 residual
  * b - A x and the FP64 solution update are refreshed on device whenever the FP32
  * residual fell by opts.reliable_delta; convergence is decided on the FP64 residual. */
@@ -234,6 +237,13 @@ int geo_forward(geo_op* op, const double* f, const geo_cg_opts* opts, double* u,
  * recomputed from f (recompute instead of store).                             */
 int geo_vjp(geo_op* op, const double* f, const double* u, const double* dJ_du,
             const geo_cg_opts* opts, double* dJ_dlncoef, geo_solver_stats* stats);
+/* Diagnostic, no reference counterpart: average device time (ms) of the two kernels
+ * of one matrix-free PCG iteration -- the patch kernel in PCG mode and the node
+ * update -- over `iterations` (1..4096) iterations started from b (original
+ * numbering, host or device), with the stopping tests disabled so that every
+ * launch does full work. CUDA events between the launches on the context stream. */
+int geo_op_time_pcg_kernels(geo_op* op, const double* b, int32_t precision, int32_t iterations,
+                            double* patch_ms, double* update_ms);
 int geo_op_destroy(geo_op* op);
 
 /* ------------------------------------------------------------------ failure detection */

@@ -97,8 +97,11 @@ def test_bench_byte_model():
     E, N = 12582912, 16974593
     # apply bytes of the 128^3 FP32 operator: E(40 + 4) + N(12 + 4 + 4) + N/8
     assert bench.apply_bytes(E, N, 4) == pytest.approx(E * 44 + N * 20 + N / 8)
-    assert bench.solve_bytes(E, N, 10, 1) == pytest.approx(10 * (bench.apply_bytes(E, N, 4) + 32 * N)
-                                                             + bench.apply_bytes(E, N, 8) + 32 * N)
+    # PCG-mode patch launch: E(40 + 4) + N(12 + 3*4 + 2*4) + N/8; node update: 7 N 4 + N/8
+    assert bench.patch_pcg_bytes(E, N, 4) == pytest.approx(E * 44 + N * 32 + N / 8)
+    assert bench.update_bytes(N, 4) == pytest.approx(28 * N + N / 8)
+    assert bench.solve_bytes(E, N, 10, 1) == pytest.approx(
+        10 * (bench.patch_pcg_bytes(E, N, 4) + bench.update_bytes(N, 4)) + bench.apply_bytes(E, N, 8) + 32 * N)
 
 
 def _gloo_worker(rank, world, port, out):
