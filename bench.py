@@ -255,6 +255,8 @@ def run_ours(args, ws, rank, local, pg):
     e2e = run_e2e(ctx, stream, mesh, k_e, mask, vals, args, dev) if not args.quick else None
     if not args.quick and rank == 0:
         extras.update(adjoint_ratio(ctx, args))
+        extras["csr_vs_matfree_64"] = csr_vs_matfree(ctx)
+        extras["elasticity_48x48x24"] = elasticity_config(ctx)
 
     # dominant kernel: the FP32 patch kernel in PCG mode, timed launch by launch with
     # CUDA events on the context stream right after the timed region
@@ -389,6 +391,91 @@ def adjoint_ratio(ctx, args):
             "adjoint_config": "48x48x32 hexes (442,368 elements, 611,585 DOFs), ln k ~ N(ln 3, 0.3^2), "
                               "1000 observation nodes, mixed precision, host-timed calls",
             "forward_s": tf, "adjoint_s": ta}
+
+
+def _device_timed(ctx, fn, reps=1):
+    """Runs fn() reps times between CUDA events on the context stream; seconds per call."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = None
+    for _ in range(reps):
+        out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps, out
+
+
+def csr_vs_matfree(ctx):
+    """64^3 cube, uniform k = 3: plain FP64 matrix-free PCG vs FP64 PCG on the
+    assembled CSR (assembly + Dirichlet elimination timed separately)."""
+    import torch
+
+    import geo_simulator_b200 as geo
+    mesh, _, mask, vals = thermal_inputs(64)
+    dm = geo.DofManager(mesh.num_nodes(), 1)
+    idx = np.nonzero(mask)[0]
+    dm.set_dirichlet(idx, vals[idx])
+    f = geo.Assembler.assemble_thermal_load(mesh, dm, Q, ctx)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    fd = torch.from_numpy(f).to(dev)
+    cg = geo.ConjugateGradient().with_tolerance(1e-8).with_max_iterations(20000)
+    geo.Assembler.assemble_thermal_stiffness_parallel(mesh, dm, 3.0, ctx)  # warm (inverse map, pattern)
+    t_asm, (Kb, fb) = _device_timed(ctx, lambda: geo.Assembler.apply_dirichlet_bcs(
+        geo.Assembler.assemble_thermal_stiffness_parallel(mesh, dm, 3.0, ctx), fd, dm, ctx))
+    cg.solve(Kb, fb)
+    t_csr, (x_csr, st_csr) = _device_timed(ctx, lambda: cg.solve(Kb, fb), 2)
+    op = geo.ThermalOperator(mesh, dm, 3.0, ctx)
+    op.solve(fb, cg)
+    t_mf, (x_mf, st_mf) = _device_timed(ctx, lambda: op.solve(fb, cg), 2)
+    return {"config": "64^3 hexes (1,572,864 elements, 2,146,689 DOFs), k = 3, Jacobi-PCG to rel-res 1e-8, FP64",
+            "csr_nnz": Kb.nnz(), "csr_assembly_and_bc_s": t_asm, "csr_pcg_s": t_csr,
+            "csr_iterations": st_csr.iterations, "matfree_pcg_s": t_mf, "matfree_iterations": st_mf.iterations,
+            "matfree_speedup_vs_csr_pcg": t_csr / t_mf,
+            "solution_rel_l2": float(torch.linalg.norm(x_mf - x_csr) / torch.linalg.norm(x_csr))}
+
+
+def elasticity_config(ctx):
+    """48x48x24 hexes of 100 x 100 x 50 km, ln E_e ~ N(ln 1e11, 0.3^2) (seed 3001),
+    nu = 0.25, rho = 3300, fixed base, roller sides: mixed and FP64 matrix-free
+    solves and the adjoint dJ/d(ln E_e) of a surface u_z misfit at 500 seeded
+    top nodes (seed 3002)."""
+    import geo_simulator_b200 as geo
+    from geo_simulator_b200.fields import choice_distinct, lognormal_field
+    lx, ly, lz = 100e3, 100e3, 50e3
+    mesh = geo.ImprovedMeshGenerator.generate_cube(48, 48, 24, lx, ly, lz)
+    N = mesh.num_nodes()
+    x, y, z = mesh.nodes[:, 0], mesh.nodes[:, 1], mesh.nodes[:, 2]
+    mask = np.zeros(3 * N, np.uint8)
+    base = np.nonzero(np.abs(z) < 1.0)[0]
+    for c in range(3):
+        mask[3 * base + c] = 1
+    mask[3 * np.nonzero((np.abs(x) < 1.0) | (np.abs(x - lx) < 1.0))[0]] = 1
+    mask[3 * np.nonzero((np.abs(y) < 1.0) | (np.abs(y - ly) < 1.0))[0] + 1] = 1
+    dm = geo.DofManager(N, 3)
+    idx = np.nonzero(mask)[0]
+    dm.set_dirichlet(idx, np.zeros(idx.size))
+    E_e = lognormal_field(3001, mesh.num_elements(), np.log(1e11), 0.3)
+    op = geo.ElasticityOperator(mesh, dm, geo.IsotropicElasticity(1e11, 0.25), E_e, ctx)
+    f = geo.Assembler.assemble_gravity_load(mesh, dm, 3300.0, [0.0, 0.0, -9.81], ctx)
+    mixed = geo.ConjugateGradient().with_tolerance(1e-8).with_max_iterations(50000).with_precision("mixed")
+    fp64 = geo.ConjugateGradient().with_tolerance(1e-8).with_max_iterations(50000)
+    op.forward(f, mixed)
+    tf, (u, sf) = _device_timed(ctx, lambda: op.forward(f, mixed))
+    t64, (u64, s64) = _device_timed(ctx, lambda: op.forward(f, fp64))
+    top = np.nonzero(np.abs(z - lz) < 1.0)[0]
+    obs = 3 * top[choice_distinct(3002, top.size, 500)] + 2
+    g = np.zeros_like(u)
+    g[obs] = u[obs] - (u[obs] + 1e-3)
+    ta, (grad, sa) = _device_timed(ctx, lambda: op.vjp(g, u=u, solver=mixed))
+    return {"config": "48x48x24 hexes (331,776 elements, 1,383,123 DOFs), mixed matrix-free PCG to rel-res 1e-8",
+            "mixed_forward_s": tf, "mixed_iterations": sf.iterations, "fp64_forward_s": t64,
+            "fp64_iterations": s64.iterations, "mixed_speedup_vs_fp64": t64 / tf,
+            "mixed_vs_fp64_rel_l2": float(np.linalg.norm(u - u64) / np.linalg.norm(u64)),
+            "adjoint_s": ta, "adjoint_forward_ratio": ta / tf, "adjoint_converged": bool(sa.converged)}
 
 
 # --------------------------------------------------------------------------- reference arm
