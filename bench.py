@@ -393,6 +393,11 @@ def adjoint_ratio(ctx, args):
             "forward_s": tf, "adjoint_s": ta}
 
 
+def _host(v):
+    """numpy view of a host array or a copy of a device tensor."""
+    return v.detach().cpu().numpy() if hasattr(v, "detach") else np.asarray(v)
+
+
 def _device_timed(ctx, fn, reps=1):
     """Runs fn() reps times between CUDA events on the context stream; seconds per call."""
     import torch
@@ -435,7 +440,7 @@ def csr_vs_matfree(ctx):
             "csr_nnz": Kb.nnz(), "csr_assembly_and_bc_s": t_asm, "csr_pcg_s": t_csr,
             "csr_iterations": st_csr.iterations, "matfree_pcg_s": t_mf, "matfree_iterations": st_mf.iterations,
             "matfree_speedup_vs_csr_pcg": t_csr / t_mf,
-            "solution_rel_l2": float(torch.linalg.norm(x_mf - x_csr) / torch.linalg.norm(x_csr))}
+            "solution_rel_l2": float(np.linalg.norm(_host(x_mf) - _host(x_csr)) / np.linalg.norm(_host(x_csr)))}
 
 
 def elasticity_config(ctx):
