@@ -163,6 +163,67 @@ __global__ void k_qdata(int phys, const double* xyz, const int32_t* conn, const 
     }
 }
 
+// Largest number of a patch's elements that touch one patch-local node. One
+// block per patch; counts in shared memory (max_local ints).
+__global__ void k_patch_maxinc(const int32_t* __restrict__ pe, const int32_t* __restrict__ po,
+                               const int32_t* __restrict__ pf, const uint32_t* __restrict__ lc, int32_t* maxinc) {
+    extern __shared__ int cnt[];
+    __shared__ int s_max;
+    const int p = blockIdx.x;
+    const int n_el = pe[p + 1] - pe[p];
+    const int nloc = (po[p + 1] - po[p]) + (pf[p + 1] - pf[p]);
+    for (int u = threadIdx.x; u < nloc; u += blockDim.x) cnt[u] = 0;
+    if (threadIdx.x == 0) s_max = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < n_el * 10; t += blockDim.x) {
+        const int j = t / 10, l = t % 10;
+        const uint32_t w = lc[((int64_t)p * 5 + l / 2) * kPatchElems + j];
+        const int u = (int)((l & 1) ? (w >> 16) : (w & 0xffffu));
+        if (u < nloc) atomicAdd(&cnt[u], 1);
+    }
+    __syncthreads();
+    int m = 0;
+    for (int u = threadIdx.x; u < nloc; u += blockDim.x) m = max(m, cnt[u]);
+    atomicMax(&s_max, m);
+    __syncthreads();
+    if (threadIdx.x == 0) maxinc[p] = s_max;
+}
+
+// max_e ||K_e||_inf per patch (row abs sums of K_e applied to the unit vectors,
+// FP64 qdata), stored as double bits: non-negative doubles order like their bits.
+template <class K>
+__global__ void k_patch_knorm(const double* __restrict__ qd64, int64_t E, double cl, double cm,
+                              unsigned long long* __restrict__ knorm) {
+    constexpr int ND = 10 * K::DPN;
+    const int64_t ne = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (ne >= E) return;
+    const double* qd = qd64 + (ne / kPatchElems) * K::NQD * kPatchElems + ne % kPatchElems;
+    double rs[ND];
+#pragma unroll
+    for (int i = 0; i < ND; ++i) rs[i] = 0.0;
+    for (int j = 0; j < ND; ++j) {
+        double x[ND], y[ND];
+#pragma unroll
+        for (int i = 0; i < ND; ++i) x[i] = i == j ? 1.0 : 0.0;
+        K::apply(qd, kPatchElems, cl, cm, x, y);
+#pragma unroll
+        for (int i = 0; i < ND; ++i) rs[i] += fabs(y[i]);
+    }
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) m = fmax(m, rs[i]);
+    atomicMax(&knorm[ne / kPatchElems], (unsigned long long)__double_as_longlong(m));
+}
+
+// bound32[p] = maxinc[p] * max_e ||K_e||_inf * 1.001 (margin for the FP32 qdata and
+// the rounding of the contributions), rounded up to FP32.
+__global__ void k_patch_bound(const int32_t* __restrict__ maxinc, const unsigned long long* __restrict__ knorm,
+                              int P, float* __restrict__ b32) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    b32[p] = __double2float_ru((double)maxinc[p] * __longlong_as_double((long long)knorm[p]) * 1.001);
+}
+
 // Diagonal of every K_e, original element order: ediag[e][dpn*l + c].
 __global__ void k_ediag(int phys, const double* xyz, const int32_t* conn, int64_t N, int64_t E, const double* coef,
                         double cl, double cm, double* ediag, int* err) {
@@ -323,6 +384,9 @@ struct geo_op {
     geo::DevBuf<uint8_t> mask_orig;  // Dirichlet mask, original DOF numbering
     geo::DevBuf<double> coef, qd64, g_new, diag_new, dinv64, ediag, diag_orig;
     geo::DevBuf<float> qd32, dinv32;
+    // per-patch bound of the FP32 fixed-point scatter (Scatter in mf_kernels.cuh)
+    geo::DevBuf<int32_t> pmaxinc;
+    geo::DevBuf<float> pbound32;
     // solver workspace
     geo::DevBuf<double> w64;
     geo::DevBuf<float> w32;
@@ -365,6 +429,7 @@ PatchView view(const geo_op* op) {
     v.foreign = op->foreign.p;
     v.lc = op->lc.p;
     v.flags = op->flags.p;
+    v.bound32 = op->pbound32.p;
     return v;
 }
 
@@ -444,6 +509,20 @@ void refresh_coefficients(geo_op* op) {
                                                               op->E, op->coef.p, op->qd64.p, op->qd32.p,
                                                               ctx->dev_err.p);
     check_launch(ctx, "k_qdata");
+    {
+        DevBuf<unsigned long long> knorm(op->n_patches);
+        GEO_CUDA(cudaMemsetAsync(knorm.p, 0, knorm.bytes(), s));
+        with_kernels(op, [&](auto k64, auto) {
+            k_patch_knorm<decltype(k64)><<<(unsigned)cdiv(op->E, 128), 128, 0, s>>>(op->qd64.p, op->E, op->cl,
+                                                                                   op->cm, knorm.p);
+        });
+        check_launch(ctx, "k_patch_knorm");
+        op->pbound32.ensure(op->n_patches);
+        k_patch_bound<<<(unsigned)cdiv(op->n_patches, 256), 256, 0, s>>>(op->pmaxinc.p, knorm.p, op->n_patches,
+                                                                         op->pbound32.p);
+        check_launch(ctx, "k_patch_bound");
+        sync(ctx, "patch bounds");
+    }
     op->ediag.ensure((size_t)op->E * 10 * op->dpn);
     k_ediag<<<(unsigned)cdiv(op->E, 128), 128, 0, s>>>(op->phys, m->xyz.p, m->conn.p, op->N, op->E, op->coef.p,
                                                        op->cl, op->cm, op->ediag.p, ctx->dev_err.p);
@@ -533,6 +612,11 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
     GEO_CUDA(cudaMemcpyAsync(&curved, aff.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     sync(ctx, "affine check");
     op->nq = curved ? 4 : 1;
+    if (op->max_local > 12288) fail(GEO_ERR_UNSUPPORTED, "patch tables exceed shared memory (too many nodes per patch)");
+    op->pmaxinc.alloc(op->n_patches);
+    k_patch_maxinc<<<(unsigned)op->n_patches, 128, (size_t)op->max_local * sizeof(int), s>>>(
+        op->pe.p, op->po.p, op->pf.p, op->lc.p, op->pmaxinc.p);
+    check_launch(ctx, "k_patch_maxinc");
     set_coef(op.get(), coef_e, coef);
     refresh_coefficients(op.get());
     with_kernels(op.get(), [&](auto k64, auto k32) {

@@ -50,7 +50,64 @@ struct PatchView {
     const int32_t* foreign;
     const uint32_t* lc;  // patch-major paired connectivity [P][5][kPatchElems]
     const uint8_t* flags;
+    // FP32 scatter bound per patch (see Scatter): (max element incidences of a
+    // patch-local node) x max_e ||K_e||_inf x 1.001, rounded up
+    const float* bound32;
 };
+
+// ------------------------------------------------------------------ shared-memory scatter
+// FP32: element contributions are accumulated in shared memory as exact
+// integers. Every contribution c of a patch is scaled by a power of two S chosen
+// so that the sum of all contributions to one DOF stays below 2^30, then rounded
+// to an INT32. Integer sums are exact, so the accumulation does not depend on the
+// order of the atomics, and INT32 shared atomics cost a fraction of FP32 ones (on
+// B200, random banks: about 3.7 SM cycles per warp operation against 13.4).
+// The bound behind S is rigorous: K_e annihilates constants (thermal) and
+// rigid translations (elasticity), so |(K_e x)_i| <= ||K_e||_inf * max_c h_c,
+// h_c = half the range of component c of x over the patch; a margin of 2^-16
+// max|x| covers the rounding of the FP32 apply, and the patch's largest number of
+// element incidences per node bounds the sum (PatchView::bound*).
+// FP64 keeps FP64 shared atomics: the drop-in path needs full FP64 accumulation.
+template <class T>
+struct Scatter;
+
+template <>
+struct Scatter<float> {
+    static constexpr bool kScaled = true;
+    static constexpr float kLim = 1073741824.0f;  // 2^30
+    __device__ __forceinline__ static float pow2_floor(float v) {
+        v = fminf(v, 1.2676506e30f);  // 2^100
+        return __uint_as_float(__float_as_uint(v) & 0x7f800000u);
+    }
+    __device__ __forceinline__ static void zero(void* acc, int slot) { static_cast<int*>(acc)[slot] = 0; }
+    __device__ __forceinline__ static void add(void* acc, int slot, float v) {
+        atomicAdd(static_cast<int*>(acc) + slot, __float2int_rn(v));
+    }
+    __device__ __forceinline__ static float get(const void* acc, int slot) {
+        return (float)static_cast<const int*>(acc)[slot];
+    }
+};
+
+template <>
+struct Scatter<double> {
+    static constexpr bool kScaled = false;
+    __device__ __forceinline__ static void zero(void* acc, int slot) { static_cast<double*>(acc)[slot] = 0.0; }
+    __device__ __forceinline__ static void add(void* acc, int slot, double v) {
+        atomicAdd(static_cast<double*>(acc) + slot, v);
+    }
+    __device__ __forceinline__ static double get(const void* acc, int slot) {
+        return static_cast<const double*>(acc)[slot];
+    }
+};
+
+// float <-> unsigned key with the same order (for warp min/max reductions)
+__device__ __forceinline__ unsigned float_key(float f) {
+    const unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
 
 // Device-resident PCG scalars.
 struct PcgState {
@@ -146,9 +203,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
     unsigned char* ebuf = smem + 16;
+    using SC = Scatter<T>;
+    const int M = pv.max_local * DPN;  // DOF slots of the patch-local table
     T* xs = reinterpret_cast<T*>(smem + patch_smem_fixed<K, T, NBUF>());
-    T* ys = xs + (size_t)pv.max_local * DPN;
-    int* snode = reinterpret_cast<int*>(ys + (size_t)pv.max_local * DPN);
+    void* ys = xs + M;  // accumulators (INT32 fixed point for FP32, FP64 otherwise), M * sizeof(T) bytes
+    int* snode = reinterpret_cast<int*>(xs + 2 * M);
+    // FP32 scatter: per component, min and max of x over the patch as order keys, by patch parity
+    __shared__ unsigned s_lo[2][DPN], s_hi[2][DPN];
     uint8_t* sfl = reinterpret_cast<uint8_t*>(snode + pv.max_local);
     T beta = T(0);
     const T* pold = nullptr;
@@ -163,6 +224,10 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     if (threadIdx.x == 0) {
         for (int b = 0; b < NBUF; ++b) mbar_init(&bar[b], 1);
         mbar_fence_init();
+        for (int c = 0; c < DPN; ++c) {
+            s_lo[0][c] = s_lo[1][c] = 0xffffffffu;
+            s_hi[0][c] = s_hi[1][c] = 0u;
+        }
     }
     __syncthreads();
     auto issue = [&](int patch, int b) {
@@ -181,6 +246,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         const int e0 = pv.pe[patch], n_el = pv.pe[patch + 1] - e0;
         const int o0 = pv.po[patch], nown = pv.po[patch + 1] - o0;
         const int f0 = pv.pf[patch], nloc = nown + pv.pf[patch + 1] - f0;
+        const float pbound = SC::kScaled ? pv.bound32[patch] : 0.0f;
+        float xlo[DPN], xhi[DPN];
+#pragma unroll
+        for (int c = 0; c < DPN; ++c) {
+            xlo[c] = 3.0e38f;
+            xhi[c] = -3.0e38f;
+        }
         // 1. gather (overlaps the bulk copies in flight); each thread issues the
         //    loads of up to kGather nodes before any store
         for (int u0 = threadIdx.x; u0 < nloc; u0 += kGather * blockDim.x) {
@@ -232,7 +304,22 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                         if (MODE == MODE_FREE ? dir : !dir) v = T(0);
                     }
                     xs[u * DPN + c] = v;
-                    ys[u * DPN + c] = T(0);
+                    if (SC::kScaled) {
+                        xlo[c] = fminf(xlo[c], (float)v);
+                        xhi[c] = fmaxf(xhi[c], (float)v);
+                    }
+                    SC::zero(ys, u * DPN + c);
+                }
+            }
+        }
+        if (SC::kScaled) {
+#pragma unroll
+            for (int c = 0; c < DPN; ++c) {
+                const unsigned lo = __reduce_min_sync(0xffffffffu, float_key(xlo[c]));
+                const unsigned hi = __reduce_max_sync(0xffffffffu, float_key(xhi[c]));
+                if ((threadIdx.x & 31) == 0) {
+                    atomicMin(&s_lo[k & 1][c], lo);
+                    atomicMax(&s_hi[k & 1][c], hi);
                 }
             }
         }
@@ -242,7 +329,28 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             if (threadIdx.x == 0) atomicOr(a.err, DEV_ERR_TIMEOUT);
             return;
         }
-        // 2. elements
+        // 2. elements (FP32: scattered as fixed-point integers with scale S, see Scatter)
+        T S = T(1), invS = T(1);
+        if (SC::kScaled) {
+            float half = 0.0f, mabs = 0.0f;
+#pragma unroll
+            for (int c = 0; c < DPN; ++c) {
+                const float lo = key_float(s_lo[k & 1][c]), hi = key_float(s_hi[k & 1][c]);
+                if (hi >= lo) {
+                    half = fmaxf(half, __fmul_ru(__fsub_ru(hi, lo), 0.5f));
+                    mabs = fmaxf(mabs, fmaxf(fabsf(lo), fabsf(hi)));
+                }
+            }
+            const float bx = __fmul_ru(pbound, __fmaf_ru(mabs, 1.52587890625e-05f, half));  // 2^-16
+            if (bx > 0.0f) {
+                S = (T)Scatter<float>::pow2_floor(Scatter<float>::kLim / bx);
+                invS = T(1) / S;
+            }
+            if (threadIdx.x < DPN) {  // next read by the patch after next
+                s_lo[(k + 1) & 1][threadIdx.x] = 0xffffffffu;
+                s_hi[(k + 1) & 1][threadIdx.x] = 0u;
+            }
+        }
         const uint32_t* lcs = reinterpret_cast<const uint32_t*>(ebuf + (size_t)b * (LCB + QDB));
         const T* qds = reinterpret_cast<const T*>(ebuf + (size_t)b * (LCB + QDB) + LCB);
         for (int el = threadIdx.x; el < n_el; el += blockDim.x) {
@@ -268,7 +376,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
 #pragma unroll
             for (int l = 0; l < 10; ++l)
 #pragma unroll
-                for (int c = 0; c < DPN; ++c) atomicAdd(&ys[li[l] * DPN + c], ye[l * DPN + c]);
+                for (int c = 0; c < DPN; ++c) SC::add(ys, li[l] * DPN + c, SC::kScaled ? ye[l * DPN + c] * S : ye[l * DPN + c]);
         }
         __syncthreads();
         if (NBUF == 1 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, 0);
@@ -280,7 +388,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
 #pragma unroll
             for (int c = 0; c < DPN; ++c) {
                 if ((fl >> c) & 1) continue;
-                const T v = ys[u * DPN + c];
+                const T v = SC::kScaled ? SC::get(ys, u * DPN + c) * invS : SC::get(ys, u * DPN + c);
                 T* dst = a.y + (int64_t)node * DPN + c;
                 if (plain) *dst = v;
                 else atomicAdd(dst, v);

@@ -103,15 +103,27 @@ def test_elasticity_vjp_vs_finite_differences(orc, geo):
     dJ = np.zeros_like(u)
     dJ[obs] = u[obs] - that[obs]
     grad, _ = op.vjp(dJ, u=u, solver=tight)  # dJ/d(ln E_e)
+
+    def J_at(lnE):
+        op.set_coefficients(np.exp(lnE))
+        up, _ = op.forward(f, tight)
+        return 0.5 * np.sum((up[obs] - that[obs]) ** 2)
+
+    # Central differences, h = 1e-6. Components far below the largest gradient
+    # are dominated by where the perturbed CG solves stop (a different iteration
+    # count moves J by the solve's error), so the per-element check takes
+    # elements whose gradient is at least 5% of the largest; a random-direction
+    # derivative covers all elements at once.
     h = 1e-6
-    for e in np.random.default_rng(9).choice(conn.shape[0], 5, replace=False):
-        vals_ = []
-        for sgn in (1, -1):
-            Ee = E_e.copy()
-            Ee[e] *= np.exp(sgn * h)
-            op.set_coefficients(Ee)
-            up, _ = op.forward(f, tight)
-            vals_.append(0.5 * np.sum((up[obs] - that[obs]) ** 2))
-        op.set_coefficients(E_e)
-        fd = (vals_[0] - vals_[1]) / (2 * h)
-        assert abs(grad[e] - fd) <= 1e-5 * max(abs(fd), 1e-3 * np.abs(grad).max()), (e, grad[e], fd)
+    lnE = np.log(E_e)
+    big = np.nonzero(np.abs(grad) >= 0.05 * np.abs(grad).max())[0]
+    for e in np.random.default_rng(9).choice(big, min(5, big.size), replace=False):
+        d = np.zeros_like(lnE)
+        d[e] = h
+        fd = (J_at(lnE + d) - J_at(lnE - d)) / (2 * h)
+        assert abs(grad[e] - fd) <= 1e-5 * abs(fd), (e, grad[e], fd)
+    d = np.random.default_rng(10).standard_normal(lnE.size)
+    d /= np.linalg.norm(d)
+    fd = (J_at(lnE + h * d) - J_at(lnE - h * d)) / (2 * h)
+    op.set_coefficients(E_e)
+    assert abs(grad @ d - fd) <= 1e-5 * abs(fd), (grad @ d, fd)
