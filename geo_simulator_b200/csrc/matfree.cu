@@ -163,6 +163,21 @@ __global__ void k_qdata(int phys, const double* xyz, const int32_t* conn, const 
     }
 }
 
+// Foreign ids and flags of every patch copied into segments that start at
+// pfa[p] (multiples of kForeignAlign entries), so that the patch kernel's bulk
+// copy brings them with the element data. One block per patch.
+__global__ void k_patch_foreign(const int32_t* __restrict__ pf, const int32_t* __restrict__ pfa,
+                               const int32_t* __restrict__ foreign, const uint8_t* __restrict__ flags,
+                               int32_t* __restrict__ fids, uint8_t* __restrict__ fflags) {
+    const int p = blockIdx.x;
+    const int f0 = pf[p], nf = pf[p + 1] - f0, a0 = pfa[p];
+    for (int k = threadIdx.x; k < nf; k += blockDim.x) {
+        const int32_t nd = foreign[f0 + k];
+        fids[a0 + k] = nd;
+        fflags[a0 + k] = flags[nd];
+    }
+}
+
 // Largest number of a patch's elements that touch one patch-local node. One
 // block per patch; counts in shared memory (max_local ints).
 __global__ void k_patch_maxinc(const int32_t* __restrict__ pe, const int32_t* __restrict__ po,
@@ -384,6 +399,10 @@ struct geo_op {
     geo::DevBuf<uint8_t> mask_orig;  // Dirichlet mask, original DOF numbering
     geo::DevBuf<double> coef, qd64, g_new, diag_new, dinv64, ediag, diag_orig;
     geo::DevBuf<float> qd32, dinv32;
+    // foreign ids and flags in aligned per-patch segments (bulk-copied with the elements)
+    geo::DevBuf<int32_t> pfa, fids;
+    geo::DevBuf<uint8_t> fflags;
+    int max_for = 0;
     // per-patch bound of the FP32 fixed-point scatter (Scatter in mf_kernels.cuh)
     geo::DevBuf<int32_t> pmaxinc;
     geo::DevBuf<float> pbound32;
@@ -430,6 +449,10 @@ PatchView view(const geo_op* op) {
     v.lc = op->lc.p;
     v.flags = op->flags.p;
     v.bound32 = op->pbound32.p;
+    v.pfa = op->pfa.p;
+    v.fids = op->fids.p;
+    v.fflags = op->fflags.p;
+    v.max_for = op->max_for;
     return v;
 }
 
@@ -437,7 +460,7 @@ PatchView view(const geo_op* op) {
 template <class K, class T>
 size_t smem_bytes(const geo_op* op, int nbuf) {
     const size_t tables = (size_t)2 * op->max_local * K::DPN * sizeof(T) + (size_t)op->max_local * 5 + 16;
-    return (nbuf == 2 ? patch_smem_fixed<K, T, 2>() : patch_smem_fixed<K, T, 1>()) + tables;
+    return (nbuf == 2 ? patch_smem_tables<K, T, 2>(op->max_for) : patch_smem_tables<K, T, 1>(op->max_for)) + tables;
 }
 
 constexpr size_t kSmemLimit = 227 * 1024;
@@ -603,6 +626,30 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
                                              op->flags.p, op->g_new.p);
     check_launch(ctx, "k_node_flags");
     sync(ctx, "operator layout");
+    {
+        const int P = op->n_patches;
+        std::vector<int32_t> pf(P + 1), pfa(P + 1);
+        GEO_CUDA(cudaMemcpy(pf.data(), op->pf.p, (P + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        int64_t acc = 0;
+        for (int p = 0; p < P; ++p) {
+            const int nfor = pf[p + 1] - pf[p];
+            op->max_for = std::max(op->max_for, nfor);
+            pfa[p] = (int32_t)acc;
+            acc += (nfor + kForeignAlign - 1) / kForeignAlign * kForeignAlign;
+        }
+        if (acc > INT32_MAX) fail(GEO_ERR_UNSUPPORTED, "too many foreign patch nodes");
+        pfa[P] = (int32_t)acc;
+        op->pfa.alloc(P + 1);
+        GEO_CUDA(cudaMemcpy(op->pfa.p, pfa.data(), (P + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+        op->fids.alloc(acc + kForeignAlign);
+        op->fflags.alloc(acc + kForeignAlign);
+        GEO_CUDA(cudaMemsetAsync(op->fids.p, 0, op->fids.bytes(), s));
+        GEO_CUDA(cudaMemsetAsync(op->fflags.p, 0, op->fflags.bytes(), s));
+        k_patch_foreign<<<(unsigned)P, 128, 0, s>>>(op->pf.p, op->pfa.p, op->foreign.p, op->flags.p, op->fids.p,
+                                                  op->fflags.p);
+        check_launch(ctx, "k_patch_foreign");
+        sync(ctx, "foreign segments");
+    }
     // affine (straight-sided) elements use one metric per element
     DevBuf<int> aff(1);
     GEO_CUDA(cudaMemsetAsync(aff.p, 0, sizeof(int), s));

@@ -2,15 +2,17 @@
 //
 // Patch apply (k_patch): a CTA works through whole patches (patch = blockIdx.x,
 // += gridDim.x). The patch's element data (16-bit local connectivity and the
-// per-element qdata, contiguous per patch) is brought into shared memory with
+// per-element qdata, contiguous per patch), its foreign node ids and flags
+// (aligned per-patch segments) and its sizes are brought into shared memory with
 // cp.async.bulk (bulk copy engine, mbarrier completion), double-buffered so the
-// next patch's copy is in flight while the current one is processed. Per patch:
+// next patch's copy is in flight while the current one is processed; the gather
+// then needs a single round trip to global memory. Per patch:
 //   1. gather: every patch-local node's input value is read once from global
 //      memory into a shared table (own nodes form one contiguous range);
 //   2. element pass: each thread applies K_e to its elements from the shared
-//      table and accumulates into a shared output table with shared atomics.
-//      Elements are ordered so a warp's 32 elements share no node, so these
-//      atomics do not collide;
+//      table and accumulates into a shared output table with shared atomics
+//      (exact INT32 fixed point for FP32, see Scatter). Elements are ordered so
+//      a warp's 32 elements share no node, so these atomics do not collide;
 //   3. flush: a plain store for nodes no other patch touches, red.global.add
 //      for the shared ones.
 // In PCG mode step 1 also forms the new search direction p = z + beta p_old
@@ -53,6 +55,13 @@ struct PatchView {
     // FP32 scatter bound per patch (see Scatter): (max element incidences of a
     // patch-local node) x max_e ||K_e||_inf x 1.001, rounded up
     const float* bound32;
+    // foreign ids and flags again, in per-patch segments that start at pfa[p]
+    // (multiples of kForeignAlign entries) so that they travel with the patch's
+    // bulk copy; max_for = the largest foreign count of a patch
+    const int32_t* pfa;
+    const int32_t* fids;
+    const uint8_t* fflags;
+    int max_for;
 };
 
 // ------------------------------------------------------------------ shared-memory scatter
@@ -189,10 +198,35 @@ __host__ __device__ constexpr uint32_t patch_bytes_lc() { return 5 * kPatchElems
 template <class K, class T>
 __host__ __device__ constexpr uint32_t patch_bytes_qd() { return K::NQD * kPatchElems * (uint32_t)sizeof(T); }
 
-// shared memory layout: [2 mbarriers | NBUF x (lc | qd) | xs | ys | node ids | flags]
+constexpr int kForeignAlign = 16;  // foreign segments start at multiples of 16 entries
+
+__host__ __device__ inline uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
+
+// A patch's sizes, written by the issuing thread next to its bulk copies.
+struct PatchMeta {
+    int n_el, o0, nown, nfor, fa;
+    float bound;  // PatchView::bound32 of the patch
+    int pad0, pad1;
+};
+
+// per-buffer bytes of [meta | foreign ids | foreign flags]
+__host__ __device__ inline uint32_t patch_aux_ids(int max_for) {
+    return round16((uint32_t)((max_for + kForeignAlign - 1) / kForeignAlign * kForeignAlign) * 4u);
+}
+__host__ __device__ inline uint32_t patch_aux_bytes(int max_for) {
+    return (uint32_t)sizeof(PatchMeta) + patch_aux_ids(max_for) +
+           round16((uint32_t)((max_for + kForeignAlign - 1) / kForeignAlign * kForeignAlign));
+}
+
+// shared memory layout: [2 mbarriers | NBUF x (lc | qd) | NBUF x (meta | foreign ids | foreign flags) |
+// xs | ys | node ids | flags]
 template <class K, class T, int NBUF>
 __host__ __device__ constexpr size_t patch_smem_fixed() {
     return 16 + (size_t)NBUF * (patch_bytes_lc<K, T>() + patch_bytes_qd<K, T>());
+}
+template <class K, class T, int NBUF>
+__host__ __device__ inline size_t patch_smem_tables(int max_for) {
+    return patch_smem_fixed<K, T, NBUF>() + (size_t)NBUF * patch_aux_bytes(max_for);
 }
 
 template <class K, class T, int MODE, int NBUF>
@@ -205,7 +239,9 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     unsigned char* ebuf = smem + 16;
     using SC = Scatter<T>;
     const int M = pv.max_local * DPN;  // DOF slots of the patch-local table
-    T* xs = reinterpret_cast<T*>(smem + patch_smem_fixed<K, T, NBUF>());
+    unsigned char* abuf = smem + patch_smem_fixed<K, T, NBUF>();  // NBUF x (meta | ids | flags)
+    const uint32_t AUX = patch_aux_bytes(pv.max_for), AIDS = patch_aux_ids(pv.max_for);
+    T* xs = reinterpret_cast<T*>(smem + patch_smem_tables<K, T, NBUF>(pv.max_for));
     void* ys = xs + M;  // accumulators (INT32 fixed point for FP32, FP64 otherwise), M * sizeof(T) bytes
     int* snode = reinterpret_cast<int*>(xs + 2 * M);
     // FP32 scatter: per component, min and max of x over the patch as order keys, by patch parity
@@ -230,11 +266,27 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         }
     }
     __syncthreads();
+    // thread 0: the patch's element data, sizes, foreign ids and foreign flags into buffer b
     auto issue = [&](int patch, int b) {
+        PatchMeta m;
+        m.n_el = pv.pe[patch + 1] - pv.pe[patch];
+        m.o0 = pv.po[patch];
+        m.nown = pv.po[patch + 1] - m.o0;
+        m.nfor = pv.pf[patch + 1] - pv.pf[patch];
+        m.fa = pv.pfa[patch];
+        m.bound = pv.bound32[patch];
+        m.pad0 = m.pad1 = 0;
+        unsigned char* ab = abuf + (size_t)b * AUX;
+        *reinterpret_cast<PatchMeta*>(ab) = m;  // published by the arrive below
+        const uint32_t ib = round16((uint32_t)m.nfor * 4u), fb = round16((uint32_t)m.nfor);
         unsigned char* dst = ebuf + (size_t)b * (LCB + QDB);
-        mbar_expect_tx(&bar[b], LCB + QDB);
+        mbar_expect_tx(&bar[b], LCB + QDB + ib + fb);
         bulk_g2s(dst, pv.lc + (size_t)patch * 5 * kPatchElems, LCB, &bar[b]);
         bulk_g2s(dst + LCB, qd_all + (size_t)patch * K::NQD * kPatchElems, QDB, &bar[b]);
+        if (ib) {
+            bulk_g2s(ab + sizeof(PatchMeta), pv.fids + m.fa, ib, &bar[b]);
+            bulk_g2s(ab + sizeof(PatchMeta) + AIDS, pv.fflags + m.fa, fb, &bar[b]);
+        }
     };
     if (threadIdx.x == 0 && blockIdx.x < pv.n_patches) issue(blockIdx.x, 0);
     uint32_t phase = 0;  // bit b = parity of buffer b
@@ -243,10 +295,19 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     for (int patch = blockIdx.x; patch < pv.n_patches; patch += gridDim.x, ++k) {
         const int b = NBUF == 2 ? (k & 1) : 0;
         if (NBUF == 2 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, b ^ 1);
-        const int e0 = pv.pe[patch], n_el = pv.pe[patch + 1] - e0;
-        const int o0 = pv.po[patch], nown = pv.po[patch + 1] - o0;
-        const int f0 = pv.pf[patch], nloc = nown + pv.pf[patch + 1] - f0;
-        const float pbound = SC::kScaled ? pv.bound32[patch] : 0.0f;
+        // the patch's sizes, element data and foreign lists (copied during the previous patch)
+        const bool ok = mbar_wait(&bar[b], (phase >> b) & 1);
+        phase ^= 1u << b;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(a.err, DEV_ERR_TIMEOUT);
+            return;
+        }
+        const unsigned char* ab = abuf + (size_t)b * AUX;
+        const PatchMeta pm = *reinterpret_cast<const PatchMeta*>(ab);
+        const int* __restrict__ sfor = reinterpret_cast<const int*>(ab + sizeof(PatchMeta));
+        const uint8_t* __restrict__ sffl = ab + sizeof(PatchMeta) + AIDS;
+        const int n_el = pm.n_el, o0 = pm.o0, nown = pm.nown, nloc = nown + pm.nfor;
+        const float pbound = pm.bound;
         float xlo[DPN], xhi[DPN];
 #pragma unroll
         for (int c = 0; c < DPN; ++c) {
@@ -262,13 +323,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
 #pragma unroll
             for (int g = 0; g < kGather; ++g) {
                 const int u = u0 + g * blockDim.x;
-                node[g] = u < nown ? o0 + u : (u < nloc ? pv.foreign[f0 + u - nown] : 0);
+                node[g] = u < nown ? o0 + u : (u < nloc ? sfor[u - nown] : 0);
             }
 #pragma unroll
             for (int g = 0; g < kGather; ++g) {
                 const int u = u0 + g * blockDim.x;
                 if (u < nloc) {
-                    fl[g] = pv.flags[node[g]];
+                    fl[g] = u < nown ? pv.flags[node[g]] : sffl[u - nown];
 #pragma unroll
                     for (int c = 0; c < DPN; ++c) {
                         const int64_t idx = (int64_t)node[g] * DPN + c;
@@ -323,12 +384,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                 }
             }
         }
-        const bool ok = mbar_wait(&bar[b], (phase >> b) & 1);
-        phase ^= 1u << b;
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicOr(a.err, DEV_ERR_TIMEOUT);
-            return;
-        }
+        __syncthreads();
         // 2. elements (FP32: scattered as fixed-point integers with scale S, see Scatter)
         T S = T(1), invS = T(1);
         if (SC::kScaled) {
