@@ -267,143 +267,6 @@ __global__ void k_apply_order(const int32_t* __restrict__ wperm, const int32_t* 
     }
 }
 
-// Bank-aware order of each patch's local node table. In the apply, a warp
-// reads and accumulates slot l (0..9) of 32 node-disjoint elements at once; the
-// 32 patch-local indices u of such a "row" hit shared-memory bank u mod 32, and
-// equal banks serialise. This kernel (one warp per patch) gives every local node
-// a bank, greedily (nodes of larger degree first; per node the bank with the
-// fewest nodes already placed in the node's rows, then the most free slots),
-// with as many own / foreign nodes per bank as the own range [0, nown) and the
-// foreign range [nown, nloc) have slots of that bank, and then numbers the nodes
-// of each bank by increasing slot. Output: lnew[po[p] + pf[p] + u] = new index of
-// local node u. The own part is a permutation of [0, nown), so only the node
-// numbering inside each patch's own range changes.
-constexpr int kRows = 10 * (kPatchElems / 32);
-
-__global__ void __launch_bounds__(32) k_bank_assign(const uint32_t* __restrict__ lc, const int32_t* __restrict__ pe,
-                                                    const int32_t* __restrict__ po, const int32_t* __restrict__ pf,
-                                                    int32_t* __restrict__ lnew) {
-    extern __shared__ int sh[];
-    const int p = blockIdx.x, lane = threadIdx.x;
-    const int n_el = pe[p + 1] - pe[p], nown = po[p + 1] - po[p], nfor = pf[p + 1] - pf[p];
-    const int nloc = nown + nfor, base = po[p] + pf[p];
-    int* cnt = sh;                     // [kRows][32]
-    int* deg = cnt + kRows * 32;       // [nloc]
-    int* off = deg + nloc;             // [nloc + 1]
-    int* fill = off + nloc + 1;        // [nloc]
-    int* list = fill + nloc;           // [10 * kPatchElems] row ids
-    int* bank = list + 10 * kPatchElems;  // [nloc]
-    int* nxt = bank + nloc;            // [64] next slot per (part, bank)
-    for (int i = lane; i < kRows * 32; i += 32) cnt[i] = 0;
-    for (int i = lane; i < nloc; i += 32) deg[i] = fill[i] = 0;
-    __syncwarp();
-    auto local = [&](int l, int j) {
-        const uint32_t w = lc[((int64_t)p * 5 + l / 2) * kPatchElems + j];
-        return (int)((l & 1) ? (w >> 16) : (w & 0xffffu));
-    };
-    for (int t = lane; t < n_el * 10; t += 32) atomicAdd(&deg[local(t % 10, t / 10)], 1);
-    __syncwarp();
-    int run = 0, maxdeg = 0;
-    for (int u0 = 0; u0 < nloc; u0 += 32) {
-        const int u = u0 + lane;
-        const int d = u < nloc ? deg[u] : 0;
-        maxdeg = max(maxdeg, d);
-        int incl = d;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        if (u < nloc) off[u] = run + incl - d;
-        run += __shfl_sync(0xffffffffu, incl, 31);
-    }
-    if (lane == 0) off[nloc] = run;
-    maxdeg = __reduce_max_sync(0xffffffffu, maxdeg);
-    __syncwarp();
-    for (int t = lane; t < n_el * 10; t += 32) {
-        const int l = t % 10, j = t / 10;
-        const int u = local(l, j);
-        list[off[u] + atomicAdd(&fill[u], 1)] = (j / 32) * 10 + l;
-    }
-    __syncwarp();
-    // lane = bank: slots of this bank in the own and in the foreign range
-    int cap_own = nown / 32 + (lane < nown % 32 ? 1 : 0);
-    const int f_first = nown + ((lane - nown % 32 + 32) % 32);
-    int cap_for = f_first < nloc ? (nloc - 1 - f_first) / 32 + 1 : 0;
-    for (int d = maxdeg; d >= 0; --d) {  // every local node gets a bank, even one no element uses
-        for (int u0 = 0; u0 < nloc; u0 += 32) {
-            unsigned m = __ballot_sync(0xffffffffu, u0 + lane < nloc && deg[u0 + lane] == d);
-            while (m) {
-                const int u = u0 + __ffs(m) - 1;
-                m &= m - 1;
-                const bool own = u < nown;
-                int c = 0;
-                for (int k = off[u]; k < off[u + 1]; ++k) c += cnt[list[k] * 32 + lane];
-                const int cap = own ? cap_own : cap_for;
-                const int key = cap > 0 ? c * 4096 + (4095 - min(cap, 4095)) : INT_MAX;
-                const int best = __reduce_min_sync(0xffffffffu, key);
-                const int b = __ffs(__ballot_sync(0xffffffffu, key == best)) - 1;
-                if (lane == b) {
-                    if (own) --cap_own;
-                    else --cap_for;
-                }
-                if (lane == 0) {
-                    bank[u] = b;
-                    for (int k = off[u]; k < off[u + 1]; ++k) ++cnt[list[k] * 32 + b];
-                }
-                __syncwarp();
-            }
-        }
-    }
-    nxt[lane] = lane;        // own range: first slot of bank `lane`
-    nxt[32 + lane] = f_first;  // foreign range
-    __syncwarp();
-    if (lane == 0)
-        for (int u = 0; u < nloc; ++u) {
-            const int slot = u < nown ? 0 : 32;
-            lnew[base + u] = nxt[slot + bank[u]];
-            nxt[slot + bank[u]] += 32;
-        }
-}
-
-// gmap[o0 + u] = o0 + lnew[u] for the own nodes of every patch (a permutation of the node ids)
-__global__ void k_bank_gmap(const int32_t* __restrict__ po, const int32_t* __restrict__ pf,
-                            const int32_t* __restrict__ lnew, int32_t* __restrict__ gmap) {
-    const int p = blockIdx.x;
-    const int o0 = po[p], nown = po[p + 1] - o0, base = po[p] + pf[p];
-    for (int u = threadIdx.x; u < nown; u += blockDim.x) gmap[o0 + u] = o0 + lnew[base + u];
-}
-
-__global__ void k_bank_nodes(const int32_t* __restrict__ gmap, const int32_t* __restrict__ nperm,
-                             const uint8_t* __restrict__ shared, int64_t N, int32_t* __restrict__ nperm2,
-                             uint8_t* __restrict__ shared2) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const int32_t j = gmap[i];
-    nperm2[j] = nperm[i];
-    shared2[j] = shared[i];
-}
-
-__global__ void k_bank_foreign(const int32_t* __restrict__ po, const int32_t* __restrict__ pf,
-                               const int32_t* __restrict__ lnew, const int32_t* __restrict__ gmap,
-                               const int32_t* __restrict__ foreign, int32_t* __restrict__ foreign2) {
-    const int p = blockIdx.x;
-    const int nown = po[p + 1] - po[p], f0 = pf[p], nfor = pf[p + 1] - f0, base = po[p] + pf[p];
-    for (int k = threadIdx.x; k < nfor; k += blockDim.x)
-        foreign2[f0 + lnew[base + nown + k] - nown] = gmap[foreign[f0 + k]];
-}
-
-__global__ void k_bank_lc(const int32_t* __restrict__ po, const int32_t* __restrict__ pf,
-                          const int32_t* __restrict__ lnew, int P, uint32_t* __restrict__ lc) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)P * 5 * kPatchElems) return;
-    const int p = (int)(t / (5 * kPatchElems));
-    const int base = po[p] + pf[p], nloc = (po[p + 1] - po[p]) + (pf[p + 1] - pf[p]);
-    const uint32_t w = lc[t];
-    const int a = (int)(w & 0xffffu), b = (int)(w >> 16);
-    const uint32_t na = a < nloc ? (uint32_t)lnew[base + a] : 0u, nb2 = b < nloc ? (uint32_t)lnew[base + b] : 0u;
-    lc[t] = na | nb2 << 16;
-}
-
 template <class F>
 void cub_call(cudaStream_t s, F&& f) {
     size_t bytes = 0;
@@ -506,30 +369,6 @@ void build_patches(cudaStream_t s, int64_t N, const double* xyz, int64_t E, cons
         GEO_CUDA(cudaGetLastError());
         GEO_CUDA(cudaStreamSynchronize(s));
         L.eperm = std::move(eperm2);
-    }
-    // ---- bank-aware order of each patch's local table (own range and foreign list)
-    const size_t bank_smem = sizeof(int) * ((size_t)kRows * 32 + 4 * (size_t)L.max_local + 1 + 10 * kPatchElems + 64);
-    if (bank_smem <= 227 * 1024) {
-        if (bank_smem > 48 * 1024)
-            GEO_CUDA(cudaFuncSetAttribute(k_bank_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bank_smem));
-        const int64_t total_local = (int64_t)N + nf;  // sum over patches of nown + nfor
-        DevBuf<int32_t> lnew(std::max<int64_t>(total_local, 1)), gmap(N), nperm2(N), foreign2(std::max<int64_t>(nf, 1));
-        DevBuf<uint8_t> shared2(N);
-        k_bank_assign<<<(unsigned)P, 32, bank_smem, s>>>(L.lc.p, L.patch_elem.p, L.patch_own.p, L.patch_foreign.p,
-                                                         lnew.p);
-        k_bank_gmap<<<(unsigned)P, 128, 0, s>>>(L.patch_own.p, L.patch_foreign.p, lnew.p, gmap.p);
-        k_bank_nodes<<<nb(N), 256, 0, s>>>(gmap.p, L.nperm.p, L.shared.p, N, nperm2.p, shared2.p);
-        if (nf > 0)
-            k_bank_foreign<<<(unsigned)P, 128, 0, s>>>(L.patch_own.p, L.patch_foreign.p, lnew.p, gmap.p, L.foreign.p,
-                                                       foreign2.p);
-        k_bank_lc<<<nb((int64_t)P * 5 * kPatchElems), 256, 0, s>>>(L.patch_own.p, L.patch_foreign.p, lnew.p, P,
-                                                                    L.lc.p);
-        k_inverse<<<nb(N), 256, 0, s>>>(nperm2.p, N, L.ninv.p);
-        GEO_CUDA(cudaGetLastError());
-        GEO_CUDA(cudaStreamSynchronize(s));
-        L.nperm = std::move(nperm2);
-        L.shared = std::move(shared2);
-        if (nf > 0) L.foreign = std::move(foreign2);
     }
 }
 

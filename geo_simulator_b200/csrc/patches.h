@@ -6,10 +6,7 @@
 // contiguous range of new node ids (the nodes it touches first); the other
 // nodes it touches ("foreign") were owned by earlier patches and are listed
 // explicitly. Connectivity is stored as 16-bit indices into the patch-local
-// node table [own range | foreign list]. Within each patch, the order of the own
-// range (the node numbering inside it) and of the foreign list is chosen so that
-// the 32 nodes a warp touches at once fall in distinct shared-memory banks where
-// possible (k_bank_assign).
+// node table [own range | foreign list].
 #pragma once
 
 #include <cstdint>
@@ -34,7 +31,7 @@ struct PatchLayout {
     DevBuf<int32_t> patch_elem;     // [n_patches + 1]
     DevBuf<int32_t> patch_own;      // [n_patches + 1] new node ids
     DevBuf<int32_t> patch_foreign;  // [n_patches + 1] offsets into foreign
-    DevBuf<int32_t> foreign;        // new node ids, in patch-local table order
+    DevBuf<int32_t> foreign;        // new node ids, ascending per patch
     // Patch-major local connectivity, two 16-bit indices per word:
     // lc[(p * 5 + l / 2) * kPatchElems + j] holds, in bits 16*(l%2).., the
     // patch-local node index of local node l of the patch's element j (entries
