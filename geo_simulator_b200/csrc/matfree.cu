@@ -403,7 +403,7 @@ struct geo_op {
     geo::DevBuf<int32_t> pfa, fids;
     geo::DevBuf<uint8_t> fflags;
     int max_for = 0;
-    // per-patch bound of the FP32 fixed-point scatter (Scatter in mf_kernels.cuh)
+    // per-patch bound of the fixed-point scatter (Scatter in mf_kernels.cuh)
     geo::DevBuf<int32_t> pmaxinc;
     geo::DevBuf<float> pbound32;
     // solver workspace
@@ -459,7 +459,9 @@ PatchView view(const geo_op* op) {
 // dynamic shared memory of the patch kernel: barriers, element-data buffers, node tables
 template <class K, class T>
 size_t smem_bytes(const geo_op* op, int nbuf) {
-    const size_t tables = (size_t)2 * op->max_local * K::DPN * sizeof(T) + (size_t)op->max_local * 5 + 16;
+    // xs (T), fixed-point accumulators (Scatter<T>::kWords INT32 words), node ids, flags
+    const size_t tables = (size_t)op->max_local * K::DPN * (sizeof(T) + 4 * Scatter<T>::kWords) +
+                          (size_t)op->max_local * 5 + 16;
     return (nbuf == 2 ? patch_smem_tables<K, T, 2>(op->max_for) : patch_smem_tables<K, T, 1>(op->max_for)) + tables;
 }
 

@@ -52,7 +52,7 @@ struct PatchView {
     const int32_t* foreign;
     const uint32_t* lc;  // patch-major paired connectivity [P][5][kPatchElems]
     const uint8_t* flags;
-    // FP32 scatter bound per patch (see Scatter): (max element incidences of a
+    // scatter bound per patch (see Scatter): (max element incidences of a
     // patch-local node) x max_e ||K_e||_inf x 1.001, rounded up
     const float* bound32;
     // foreign ids and flags again, in per-patch segments that start at pfa[p]
@@ -65,49 +65,65 @@ struct PatchView {
 };
 
 // ------------------------------------------------------------------ shared-memory scatter
-// FP32: element contributions are accumulated in shared memory as exact
-// integers. Every contribution c of a patch is scaled by a power of two S chosen
-// so that the sum of all contributions to one DOF stays below 2^30, then rounded
-// to an INT32. Integer sums are exact, so the accumulation does not depend on the
-// order of the atomics, and INT32 shared atomics cost a fraction of FP32 ones (on
-// B200, random banks: about 3.7 SM cycles per warp operation against 13.4).
+// Element contributions are accumulated in shared memory as exact integers.
+// Every contribution c of a patch is scaled by a power of two S chosen so that
+// the sum of all contributions to one DOF stays below kLim, then rounded to an
+// integer held in kWords INT32 words. Integer sums are exact, so the
+// accumulation does not depend on the order of the atomics, and INT32 shared
+// atomics cost a fraction of FP32 / FP64 ones (on B200, random banks: about 3.7
+// SM cycles per warp operation against 13.4 for FP32 and 22 for FP64).
 // The bound behind S is rigorous: K_e annihilates constants (thermal) and
 // rigid translations (elasticity), so |(K_e x)_i| <= ||K_e||_inf * max_c h_c,
 // h_c = half the range of component c of x over the patch; a margin of 2^-16
-// max|x| covers the rounding of the FP32 apply, and the patch's largest number of
-// element incidences per node bounds the sum (PatchView::bound*).
-// FP64 keeps FP64 shared atomics: the drop-in path needs full FP64 accumulation.
+// max|x| covers the rounding of the apply, and the patch's largest number of
+// element incidences per node bounds the sum (PatchView::bound32).
+// FP32: one word (|sum| < 2^30, resolution 2^-30 of the bound). FP64: three
+// words holding hi 2^42 + mid 2^21 + lo (|sum| < 2^62, resolution 2^-62 of the
+// bound, below the FP64 rounding of the result). Word w of DOF slot s sits at
+// acc[w * m + s].
 template <class T>
 struct Scatter;
 
 template <>
 struct Scatter<float> {
-    static constexpr bool kScaled = true;
     static constexpr float kLim = 1073741824.0f;  // 2^30
-    __device__ __forceinline__ static float pow2_floor(float v) {
-        v = fminf(v, 1.2676506e30f);  // 2^100
-        return __uint_as_float(__float_as_uint(v) & 0x7f800000u);
+    static constexpr int kWords = 1;
+    __device__ __forceinline__ static void zero(int* acc, int, int slot) { acc[slot] = 0; }
+    __device__ __forceinline__ static void add(int* acc, int, int slot, float v) {
+        atomicAdd(acc + slot, __float2int_rn(v));
     }
-    __device__ __forceinline__ static void zero(void* acc, int slot) { static_cast<int*>(acc)[slot] = 0; }
-    __device__ __forceinline__ static void add(void* acc, int slot, float v) {
-        atomicAdd(static_cast<int*>(acc) + slot, __float2int_rn(v));
-    }
-    __device__ __forceinline__ static float get(const void* acc, int slot) {
-        return (float)static_cast<const int*>(acc)[slot];
-    }
+    __device__ __forceinline__ static float get(const int* acc, int, int slot) { return (float)acc[slot]; }
 };
 
 template <>
 struct Scatter<double> {
-    static constexpr bool kScaled = false;
-    __device__ __forceinline__ static void zero(void* acc, int slot) { static_cast<double*>(acc)[slot] = 0.0; }
-    __device__ __forceinline__ static void add(void* acc, int slot, double v) {
-        atomicAdd(static_cast<double*>(acc) + slot, v);
+    static constexpr float kLim = 4.611686018427388e18f;  // 2^62
+    static constexpr int kWords = 3;
+    __device__ __forceinline__ static void zero(int* acc, int m, int slot) {
+        acc[slot] = 0;
+        acc[m + slot] = 0;
+        acc[2 * m + slot] = 0;
     }
-    __device__ __forceinline__ static double get(const void* acc, int slot) {
-        return static_cast<const double*>(acc)[slot];
+    // v = hi 2^42 + mid 2^21 + lo; hi and mid are exact, lo rounds the last fraction
+    __device__ __forceinline__ static void add(int* acc, int m, int slot, double v) {
+        const int hi = __double2int_rn(v * 2.2737367544323206e-13);  // 2^-42
+        const double r = fma(-(double)hi, 4398046511104.0, v);         // 2^42, exact
+        const int mid = __double2int_rn(r * 4.76837158203125e-07);    // 2^-21
+        const int lo = __double2int_rn(fma(-(double)mid, 2097152.0, r));
+        atomicAdd(acc + slot, hi);
+        atomicAdd(acc + m + slot, mid);
+        atomicAdd(acc + 2 * m + slot, lo);
+    }
+    __device__ __forceinline__ static double get(const int* acc, int m, int slot) {
+        return fma((double)acc[slot], 4398046511104.0, fma((double)acc[m + slot], 2097152.0, (double)acc[2 * m + slot]));
     }
 };
+
+// power of two <= v (v > 0), clamped to [2^-100, 2^100]
+__device__ __forceinline__ float pow2_floor(float v) {
+    v = fminf(fmaxf(v, 7.888609e-31f), 1.2676506e30f);
+    return __uint_as_float(__float_as_uint(v) & 0x7f800000u);
+}
 
 // float <-> unsigned key with the same order (for warp min/max reductions)
 __device__ __forceinline__ unsigned float_key(float f) {
@@ -242,8 +258,8 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     unsigned char* abuf = smem + patch_smem_fixed<K, T, NBUF>();  // NBUF x (meta | ids | flags)
     const uint32_t AUX = patch_aux_bytes(pv.max_for), AIDS = patch_aux_ids(pv.max_for);
     T* xs = reinterpret_cast<T*>(smem + patch_smem_tables<K, T, NBUF>(pv.max_for));
-    void* ys = xs + M;  // accumulators (INT32 fixed point for FP32, FP64 otherwise), M * sizeof(T) bytes
-    int* snode = reinterpret_cast<int*>(xs + 2 * M);
+    int* ys = reinterpret_cast<int*>(xs + M);  // fixed-point accumulators, SC::kWords x M words
+    int* snode = ys + SC::kWords * M;
     // FP32 scatter: per component, min and max of x over the patch as order keys, by patch parity
     __shared__ unsigned s_lo[2][DPN], s_hi[2][DPN];
     uint8_t* sfl = reinterpret_cast<uint8_t*>(snode + pv.max_local);
@@ -365,15 +381,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                         if (MODE == MODE_FREE ? dir : !dir) v = T(0);
                     }
                     xs[u * DPN + c] = v;
-                    if (SC::kScaled) {
-                        xlo[c] = fminf(xlo[c], (float)v);
-                        xhi[c] = fmaxf(xhi[c], (float)v);
-                    }
-                    SC::zero(ys, u * DPN + c);
+                    xlo[c] = fminf(xlo[c], (float)v);
+                    xhi[c] = fmaxf(xhi[c], (float)v);
+                    SC::zero(ys, M, u * DPN + c);
                 }
             }
         }
-        if (SC::kScaled) {
+        {
 #pragma unroll
             for (int c = 0; c < DPN; ++c) {
                 const unsigned lo = __reduce_min_sync(0xffffffffu, float_key(xlo[c]));
@@ -385,9 +399,9 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             }
         }
         __syncthreads();
-        // 2. elements (FP32: scattered as fixed-point integers with scale S, see Scatter)
+        // 2. elements, scattered as fixed-point integers with scale S (see Scatter)
         T S = T(1), invS = T(1);
-        if (SC::kScaled) {
+        {
             float half = 0.0f, mabs = 0.0f;
 #pragma unroll
             for (int c = 0; c < DPN; ++c) {
@@ -399,7 +413,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             }
             const float bx = __fmul_ru(pbound, __fmaf_ru(mabs, 1.52587890625e-05f, half));  // 2^-16
             if (bx > 0.0f) {
-                S = (T)Scatter<float>::pow2_floor(Scatter<float>::kLim / bx);
+                S = (T)pow2_floor(SC::kLim / bx);
                 invS = T(1) / S;
             }
             if (threadIdx.x < DPN) {  // next read by the patch after next
@@ -432,7 +446,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
 #pragma unroll
             for (int l = 0; l < 10; ++l)
 #pragma unroll
-                for (int c = 0; c < DPN; ++c) SC::add(ys, li[l] * DPN + c, SC::kScaled ? ye[l * DPN + c] * S : ye[l * DPN + c]);
+                for (int c = 0; c < DPN; ++c) SC::add(ys, M, li[l] * DPN + c, ye[l * DPN + c] * S);
         }
         __syncthreads();
         if (NBUF == 1 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, 0);
@@ -444,7 +458,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
 #pragma unroll
             for (int c = 0; c < DPN; ++c) {
                 if ((fl >> c) & 1) continue;
-                const T v = SC::kScaled ? SC::get(ys, u * DPN + c) * invS : SC::get(ys, u * DPN + c);
+                const T v = SC::get(ys, M, u * DPN + c) * invS;
                 T* dst = a.y + (int64_t)node * DPN + c;
                 if (plain) *dst = v;
                 else atomicAdd(dst, v);
