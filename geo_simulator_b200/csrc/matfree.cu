@@ -415,7 +415,7 @@ struct geo_op {
     geo::PcgState* h_state = nullptr;  // pinned mirror
     int patch_grid[2] = {0, 0};        // resident patch-kernel blocks (FP64, FP32)
     int nbuf[2] = {2, 2};              // element-data buffers of the patch kernel (FP64, FP32)
-    int node_grid = 0;
+    int node_grid[2] = {0, 0};  // resident node-kernel blocks (FP64, mixed)
     // CUDA graphs of PCG iteration chunks, keyed by precision
     cudaGraphExec_t chunk[2] = {nullptr, nullptr};
     const void* chunk_key[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -674,11 +674,19 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
         op->patch_grid[0] = setup_patch_kernels<K64, double>(op.get(), 0);
         op->patch_grid[1] = setup_patch_kernels<K32, float>(op.get(), 1);
     });
-    op->node_grid = ctx->sm_count * 8;
+    with_kernels(op.get(), [&](auto k64, auto k32) {
+        int per_sm = 0;
+        GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, k_pcg_update<double, decltype(k64)::DPN, false>, kNodeBS, 0));
+        op->node_grid[0] = std::max(1, per_sm) * ctx->sm_count;
+        GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, k_pcg_update<float, decltype(k32)::DPN, true>, kNodeBS, 0));
+        op->node_grid[1] = std::max(1, per_sm) * ctx->sm_count;
+    });
     op->bvec.alloc(op->ndof);
     op->xvec.alloc(op->ndof);
     op->state.alloc(1);
-    op->part.alloc((size_t)2 * std::max({op->patch_grid[0], op->patch_grid[1], op->node_grid}));
+    op->part.alloc((size_t)2 * std::max({op->patch_grid[0], op->patch_grid[1], op->node_grid[0], op->node_grid[1]}));
     GEO_CUDA(cudaMemset(op->state.p, 0, sizeof(PcgState)));
     GEO_CUDA(cudaMallocHost(&op->h_state, sizeof(PcgState)));
     return op.release();
@@ -739,7 +747,7 @@ void enqueue_iteration(geo_op* op, cudaStream_t s, const PatchArgs<T>& pa, const
     constexpr bool dbl = std::is_same<T, double>::value;
     const T* qd = dbl ? (const T*)op->qd64.p : (const T*)op->qd32.p;
     launch_patch<K, T, MODE_PCG>(op, dbl ? 0 : 1, s, qd, pa);
-    k_pcg_update<T, K::DPN, MIXED><<<(unsigned)op->node_grid, kNodeBS, 0, s>>>(na);
+    k_pcg_update<T, K::DPN, MIXED><<<(unsigned)op->node_grid[dbl ? 0 : 1], kNodeBS, 0, s>>>(na);
 }
 
 // Kernel arguments of the PCG loop over the operator's workspace (FP64 mode: r, q,
@@ -753,8 +761,11 @@ struct PcgLaunchArgs {
 
 PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
     const int64_t n = op->ndof;
-    op->w64.ensure((size_t)(mixed ? 1 : 4) * n);
-    if (mixed) op->w32.ensure((size_t)5 * n);
+    // sub-arrays at a common stride of whole 256-byte blocks, so that all vectors of
+    // the node update share 16-byte alignment
+    const int64_t np = (n + 63) / 64 * 64;
+    op->w64.ensure((size_t)(mixed ? 1 : 4) * np);
+    if (mixed) op->w32.ensure((size_t)5 * np);
     PcgLaunchArgs a;
     NodeArgs<double>& n64 = a.n64;
     NodeArgs<float>& n32 = a.n32;
@@ -772,9 +783,9 @@ PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
     if (!mixed) {
         n64.x = op->xvec.p;
         n64.r = op->w64.p;
-        n64.q = op->w64.p + n;
-        n64.pbuf0 = op->w64.p + 2 * n;
-        n64.pbuf1 = op->w64.p + 3 * n;
+        n64.q = op->w64.p + np;
+        n64.pbuf0 = op->w64.p + 2 * np;
+        n64.pbuf1 = op->w64.p + 3 * np;
         n64.dinv = op->dinv64.p;
         p64.r = n64.r;
         p64.dinv = n64.dinv;
@@ -784,10 +795,10 @@ PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
     } else {
         n32.w64 = op->w64.p;
         n32.x = op->w32.p;
-        n32.r = op->w32.p + n;
-        n32.q = op->w32.p + 2 * n;
-        n32.pbuf0 = op->w32.p + 3 * n;
-        n32.pbuf1 = op->w32.p + 4 * n;
+        n32.r = op->w32.p + np;
+        n32.q = op->w32.p + 2 * np;
+        n32.pbuf0 = op->w32.p + 3 * np;
+        n32.pbuf1 = op->w32.p + 4 * np;
         n32.dinv = op->dinv32.p;
         p32.r = n32.r;
         p32.dinv = n32.dinv;
@@ -795,6 +806,9 @@ PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
         p32.pbuf1 = n32.pbuf1;
         p32.y = n32.q;
     }
+    auto al = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };
+    n64.vec = al(n64.x) && al(n64.r) && al(n64.q) && al(n64.dinv) && al(n64.pbuf0) && al(n64.pbuf1);
+    n32.vec = al(n32.x) && al(n32.r) && al(n32.q) && al(n32.dinv) && al(n32.pbuf0) && al(n32.pbuf1);
     return a;
 }
 
@@ -802,7 +816,7 @@ PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
 void pcg_start(geo_op* op, bool mixed, const PcgState& init, const PcgLaunchArgs& a) {
     cudaStream_t s = op->ctx->stream;
     GEO_CUDA(cudaMemcpyAsync(op->state.p, &init, sizeof(init), cudaMemcpyHostToDevice, s));
-    const unsigned ng = (unsigned)op->node_grid;
+    const unsigned ng = (unsigned)op->node_grid[mixed ? 1 : 0];
     if (mixed) {
         k_mixed_init1<<<ng, kNodeBS, 0, s>>>(a.n32);
         k_mixed_init2<<<ng, kNodeBS, 0, s>>>(a.n32);
@@ -833,7 +847,7 @@ int solve_new(geo_op* op, const geo_cg_opts& o, geo_solver_stats* st) {
     const PatchArgs<double>& p64 = la.p64;
     const PatchArgs<float>& p32 = la.p32;
     const NodeArgs<double>& n64 = la.n64;
-    const unsigned ng = (unsigned)op->node_grid;
+    const unsigned ng = (unsigned)op->node_grid[mixed ? 1 : 0];
     GEO_CUDA(cudaEventRecord(ctx->ev0, s));
     pcg_start(op, mixed, init, la);
     // (re)build the chunk graph when the buffers it captured changed
@@ -924,7 +938,7 @@ void time_iterations(geo_op* op, bool mixed, int iters, double* patch_ms, double
         }
     } guard{ev};
     for (auto& e : ev) GEO_CUDA(cudaEventCreate(&e));
-    const unsigned ng = (unsigned)op->node_grid;
+    const unsigned ng = (unsigned)op->node_grid[mixed ? 1 : 0];
     with_kernels(op, [&](auto k64, auto k32) {
         for (int i = 0; i < iters; ++i) {
             GEO_CUDA(cudaEventRecord(ev[2 * i], s));

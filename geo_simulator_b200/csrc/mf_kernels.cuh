@@ -505,9 +505,26 @@ struct NodeArgs {
     double* x64;
     double* w64;
     const double* b;
+    int vec;  // x, r, q, dinv, pbuf0 and pbuf1 are 16-byte aligned: k_pcg_update uses 16-byte loads
+};
+
+// 16-byte vector of T
+template <class T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using type = float4;
+    static constexpr int N = 4;
+};
+template <>
+struct Vec16<double> {
+    using type = double2;
+    static constexpr int N = 2;
 };
 
 // x += alpha p, r -= alpha q, z = D^-1 r; r.r and r.z; stopping / refresh decision.
+// With aligned vectors (a.vec) every thread streams 16-byte loads of p, q, x, r
+// and D^-1, kUnroll vectors in flight, and a scalar loop covers the tail.
 template <class T, int DPN, bool MIXED>
 __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
     PcgState* st = a.st;
@@ -520,46 +537,70 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
     T* __restrict__ x = a.x;
     T* __restrict__ r = a.r;
     T* __restrict__ q = a.q;
+    using VT = typename Vec16<T>::type;
+    constexpr int V = Vec16<T>::N;
     const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     T acc_rr = T(0), acc_rz = T(0);
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    for (; i + (kUnroll - 1) * nth < n; i += kUnroll * nth) {
-        uint8_t fl[kUnroll];
-        T pj[kUnroll], qj[kUnroll], xj[kUnroll], rj[kUnroll], dj[kUnroll];
+    // one entry: new x and r, q zeroed where another patch accumulates into it next time
+    auto entry = [&](int64_t j, T pj, T qj, T xj, T rj, T dj, T& xo, T& ro) {
+        const uint8_t f = flags[j / DPN];
+        const bool dir = (f >> (j % DPN)) & 1;
+        const T qq = dir ? cd * pj : qj;
+        if (!dir && (f & kFlagShared)) q[j] = T(0);
+        xo = xj + alpha * pj;
+        ro = rj - alpha * qq;
+        acc_rr += ro * ro;
+        acc_rz += ro * (ro * dj);
+    };
+    const int64_t nv = a.vec ? n / V : 0;
+    int64_t iv = tid;
+    for (; iv + (kUnroll - 1) * nth < nv; iv += kUnroll * nth) {
+        VT pv[kUnroll], qv[kUnroll], xv[kUnroll], rv[kUnroll], dv[kUnroll];
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
-            const int64_t j = i + u * nth;
-            fl[u] = flags[j / DPN];
-            pj[u] = p[j];
-            qj[u] = q[j];
-            xj[u] = x[j];
-            rj[u] = r[j];
-            dj[u] = dinv[j];
+            const int64_t k = iv + u * nth;
+            pv[u] = reinterpret_cast<const VT*>(p)[k];
+            qv[u] = reinterpret_cast<const VT*>(q)[k];
+            xv[u] = reinterpret_cast<const VT*>(x)[k];
+            rv[u] = reinterpret_cast<const VT*>(r)[k];
+            dv[u] = reinterpret_cast<const VT*>(dinv)[k];
         }
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
-            const int64_t j = i + u * nth;
-            const bool dir = (fl[u] >> (j % DPN)) & 1;
-            const T qq = dir ? cd * pj[u] : qj[u];
-            if (!dir && (fl[u] & kFlagShared)) q[j] = T(0);
-            x[j] = xj[u] + alpha * pj[u];
-            const T rr = rj[u] - alpha * qq;
-            r[j] = rr;
-            acc_rr += rr * rr;
-            acc_rz += rr * (rr * dj[u]);
+            const int64_t k = iv + u * nth;
+            const T* pe = reinterpret_cast<const T*>(&pv[u]);
+            const T* qe = reinterpret_cast<const T*>(&qv[u]);
+            const T* xe = reinterpret_cast<const T*>(&xv[u]);
+            const T* re = reinterpret_cast<const T*>(&rv[u]);
+            const T* de = reinterpret_cast<const T*>(&dv[u]);
+            VT xo, ro;
+            T* xoe = reinterpret_cast<T*>(&xo);
+            T* roe = reinterpret_cast<T*>(&ro);
+#pragma unroll
+            for (int e = 0; e < V; ++e) entry(k * V + e, pe[e], qe[e], xe[e], re[e], de[e], xoe[e], roe[e]);
+            reinterpret_cast<VT*>(x)[k] = xo;
+            reinterpret_cast<VT*>(r)[k] = ro;
         }
     }
-    for (; i < n; i += nth) {
-        const uint8_t f = flags[i / DPN];
-        const bool dir = (f >> (i % DPN)) & 1;
-        const T pj = p[i];
-        const T qq = dir ? cd * pj : q[i];
-        if (!dir && (f & kFlagShared)) q[i] = T(0);
-        x[i] += alpha * pj;
-        const T rr = r[i] - alpha * qq;
-        r[i] = rr;
-        acc_rr += rr * rr;
-        acc_rz += rr * (rr * dinv[i]);
+    for (; iv < nv; iv += nth) {
+        const VT pv = reinterpret_cast<const VT*>(p)[iv], qv = reinterpret_cast<const VT*>(q)[iv];
+        const VT xv = reinterpret_cast<const VT*>(x)[iv], rv = reinterpret_cast<const VT*>(r)[iv];
+        const VT dv = reinterpret_cast<const VT*>(dinv)[iv];
+        VT xo, ro;
+#pragma unroll
+        for (int e = 0; e < V; ++e)
+            entry(iv * V + e, reinterpret_cast<const T*>(&pv)[e], reinterpret_cast<const T*>(&qv)[e],
+                  reinterpret_cast<const T*>(&xv)[e], reinterpret_cast<const T*>(&rv)[e],
+                  reinterpret_cast<const T*>(&dv)[e], reinterpret_cast<T*>(&xo)[e], reinterpret_cast<T*>(&ro)[e]);
+        reinterpret_cast<VT*>(x)[iv] = xo;
+        reinterpret_cast<VT*>(r)[iv] = ro;
+    }
+    for (int64_t j = nv * V + tid; j < n; j += nth) {
+        T xo, ro;
+        entry(j, p[j], q[j], x[j], r[j], dinv[j], xo, ro);
+        x[j] = xo;
+        r[j] = ro;
     }
     double v[2] = {(double)acc_rr, (double)acc_rz};
     store_partial<2>(a.part, v);
