@@ -410,6 +410,11 @@ struct geo_op {
     geo::DevBuf<double> w64;
     geo::DevBuf<float> w32;
     geo::DevBuf<double> bvec, xvec;  // right-hand side and solution (patch numbering)
+    // grow-only temporaries of the API calls (no cudaMalloc / cudaFree per call once
+    // grown: cudaFree synchronises the device and can stall the caller)
+    geo::DevBuf<double> tmp[7];
+    geo::DevBuf<float> tmp32[2];
+    geo::DevBuf<unsigned long long> tmpu[2];
     geo::DevBuf<geo::PcgState> state;
     geo::DevBuf<double> part;
     geo::PcgState* h_state = nullptr;  // pinned mirror
@@ -433,6 +438,12 @@ constexpr int kChunk = 16;  // PCG iterations per graph launch
 
 inline unsigned nblk(int64_t n, int bs = 256) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, bs), 148 * 64));
+}
+
+template <class T>
+T* grow(DevBuf<T>& b, size_t n) {
+    b.ensure(n);
+    return b.p;
 }
 
 PatchView view(const geo_op* op) {
@@ -535,15 +546,15 @@ void refresh_coefficients(geo_op* op) {
                                                               ctx->dev_err.p);
     check_launch(ctx, "k_qdata");
     {
-        DevBuf<unsigned long long> knorm(op->n_patches);
-        GEO_CUDA(cudaMemsetAsync(knorm.p, 0, knorm.bytes(), s));
+        unsigned long long* knorm = grow(op->tmpu[0], (size_t)op->n_patches);
+        GEO_CUDA(cudaMemsetAsync(knorm, 0, (size_t)op->n_patches * sizeof(unsigned long long), s));
         with_kernels(op, [&](auto k64, auto) {
             k_patch_knorm<decltype(k64)><<<(unsigned)cdiv(op->E, 128), 128, 0, s>>>(op->qd64.p, op->E, op->cl,
-                                                                                   op->cm, knorm.p);
+                                                                                   op->cm, knorm);
         });
         check_launch(ctx, "k_patch_knorm");
         op->pbound32.ensure(op->n_patches);
-        k_patch_bound<<<(unsigned)cdiv(op->n_patches, 256), 256, 0, s>>>(op->pmaxinc.p, knorm.p, op->n_patches,
+        k_patch_bound<<<(unsigned)cdiv(op->n_patches, 256), 256, 0, s>>>(op->pmaxinc.p, knorm, op->n_patches,
                                                                          op->pbound32.p);
         check_launch(ctx, "k_patch_bound");
         sync(ctx, "patch bounds");
@@ -557,12 +568,12 @@ void refresh_coefficients(geo_op* op) {
     k_gather_diag<<<(unsigned)cdiv(op->ndof, 256), 256, 0, s>>>(m->inc_ptr.p, m->inc.p, op->ediag.p, op->N,
                                                                 op->dpn, op->diag_orig.p);
     check_launch(ctx, "k_gather_diag");
-    DevBuf<unsigned long long> mx(1);
-    GEO_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(unsigned long long), s));
-    k_max_abs<<<nblk(op->ndof), 256, 0, s>>>(op->diag_orig.p, op->ndof, mx.p);
+    unsigned long long* mx = grow(op->tmpu[1], 1);
+    GEO_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned long long), s));
+    k_max_abs<<<nblk(op->ndof), 256, 0, s>>>(op->diag_orig.p, op->ndof, mx);
     check_launch(ctx, "k_max_abs");
     unsigned long long bits = 0;
-    GEO_CUDA(cudaMemcpyAsync(&bits, mx.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    GEO_CUDA(cudaMemcpyAsync(&bits, mx, sizeof(bits), cudaMemcpyDeviceToHost, s));
     sync(ctx, "char_diag");
     double maxd;
     std::memcpy(&maxd, &bits, sizeof(double));
@@ -732,10 +743,11 @@ void to_orig(geo_op* op, const double* in_new, double* out_orig) {
 // f_bc (patch numbering) from f (original numbering), device buffers
 void lift_new(geo_op* op, const double* f_orig_dev, double* fbc_new) {
     cudaStream_t s = op->ctx->stream;
-    DevBuf<double> fn(op->ndof), kg(op->ndof);
-    to_new(op, f_orig_dev, fn.p);
-    apply_new<double>(op, op->g_new.p, kg.p, MODE_LIFT);
-    k_lift_finish<<<nblk(op->ndof), 256, 0, s>>>(op->flags.p, op->dpn, op->ndof, op->cd, fn.p, op->g_new.p, kg.p,
+    double* fn = grow(op->tmp[4], (size_t)op->ndof);
+    double* kg = grow(op->tmp[5], (size_t)op->ndof);
+    to_new(op, f_orig_dev, fn);
+    apply_new<double>(op, op->g_new.p, kg, MODE_LIFT);
+    k_lift_finish<<<nblk(op->ndof), 256, 0, s>>>(op->flags.p, op->dpn, op->ndof, op->cd, fn, op->g_new.p, kg,
                                                 fbc_new);
     check_launch(op->ctx, "k_lift_finish");
     sync(op->ctx, "lift");
@@ -1026,21 +1038,24 @@ int geo_op_apply(geo_op* op, const double* x, double* y, int32_t precision) {
     GEO_CHECK_ARG(op && x && y, "NULL argument");
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
-    DevBuf<double> tx, xn(n), yn(n), yo(n);
-    const double* dx = stage_in(x, n, tx, s);
-    to_new(op, dx, xn.p);
+    const double* dx = stage_in(x, n, op->tmp[0], s);
+    double* yo = grow(op->tmp[3], (size_t)n);
     if (precision == GEO_PRECISION_MIXED) {
-        DevBuf<float> x32(n), y32(n);
-        k_to_new<double, float><<<nblk(n), 256, 0, s>>>(op->nperm.p, op->dpn, op->N, dx, x32.p);
-        apply_new<float>(op, x32.p, y32.p, MODE_FREE);
-        k_to_orig<float, double><<<nblk(n), 256, 0, s>>>(op->nperm.p, op->dpn, op->N, y32.p, yo.p);
+        float* x32 = grow(op->tmp32[0], (size_t)n);
+        float* y32 = grow(op->tmp32[1], (size_t)n);
+        k_to_new<double, float><<<nblk(n), 256, 0, s>>>(op->nperm.p, op->dpn, op->N, dx, x32);
+        apply_new<float>(op, x32, y32, MODE_FREE);
+        k_to_orig<float, double><<<nblk(n), 256, 0, s>>>(op->nperm.p, op->dpn, op->N, y32, yo);
         check_launch(op->ctx, "k_to_orig");
-        copy_out(y, yo.p, n, s);
+        copy_out(y, yo, n, s);
         sync(op->ctx, "geo_op_apply");
     } else {
-        apply_new<double>(op, xn.p, yn.p, MODE_FREE);
-        to_orig(op, yn.p, yo.p);
-        copy_out(y, yo.p, n, s);
+        double* xn = grow(op->tmp[1], (size_t)n);
+        double* yn = grow(op->tmp[2], (size_t)n);
+        to_new(op, dx, xn);
+        apply_new<double>(op, xn, yn, MODE_FREE);
+        to_orig(op, yn, yo);
+        copy_out(y, yo, n, s);
         sync(op->ctx, "geo_op_apply");
     }
     GEO_API_END
@@ -1051,11 +1066,12 @@ int geo_op_lift_rhs(geo_op* op, const double* f, double* f_bc) {
     GEO_CHECK_ARG(op && f && f_bc, "NULL argument");
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
-    DevBuf<double> tf, fb(n), fo(n);
-    const double* df = stage_in(f, n, tf, s);
-    lift_new(op, df, fb.p);
-    to_orig(op, fb.p, fo.p);
-    copy_out(f_bc, fo.p, n, s);
+    const double* df = stage_in(f, n, op->tmp[0], s);
+    double* fb = grow(op->tmp[1], (size_t)n);
+    double* fo = grow(op->tmp[2], (size_t)n);
+    lift_new(op, df, fb);
+    to_orig(op, fb, fo);
+    copy_out(f_bc, fo, n, s);
     sync(op->ctx, "geo_op_lift_rhs");
     GEO_API_END
 }
@@ -1063,9 +1079,9 @@ int geo_op_lift_rhs(geo_op* op, const double* f, double* f_bc) {
 int geo_op_diagonal(geo_op* op, double* diag) {
     GEO_API_BEGIN(op ? op->ctx : nullptr)
     GEO_CHECK_ARG(op && diag, "NULL argument");
-    DevBuf<double> d(op->ndof);
-    to_orig(op, op->diag_new.p, d.p);
-    copy_out(diag, d.p, op->ndof, op->ctx->stream);
+    double* d = grow(op->tmp[0], (size_t)op->ndof);
+    to_orig(op, op->diag_new.p, d);
+    copy_out(diag, d, op->ndof, op->ctx->stream);
     sync(op->ctx, "geo_op_diagonal");
     GEO_API_END
 }
@@ -1077,15 +1093,11 @@ int geo_cg_solve_matfree(geo_op* op, const double* b, const geo_cg_opts* opts, d
     cg_opts_fill(opts, o);
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
-    DevBuf<double> tb, xo;
-    const double* db = stage_in(b, n, tb, s);
+    const double* db = stage_in(b, n, op->tmp[0], s);
     to_new(op, db, op->bvec.p);
     const int status = solve_new(op, o, st);
     double* dst = x;
-    if (!is_device_ptr(x)) {
-        xo.alloc(n);
-        dst = xo.p;
-    }
+    if (!is_device_ptr(x)) dst = grow(op->tmp[1], (size_t)n);
     to_orig(op, op->xvec.p, dst);
     if (dst != x) copy_out(x, dst, n, s);
     sync(op->ctx, "geo_cg_solve_matfree");
@@ -1097,15 +1109,15 @@ int geo_op_element_gradient(geo_op* op, const double* u, const double* lambda, d
     GEO_API_BEGIN(op ? op->ctx : nullptr)
     GEO_CHECK_ARG(op && u && lambda && grad_e, "NULL argument");
     cudaStream_t s = op->ctx->stream;
-    DevBuf<double> tu, tl, g(op->E);
-    const double* du = stage_in(u, op->ndof, tu, s);
-    const double* dl = stage_in(lambda, op->ndof, tl, s);
+    const double* du = stage_in(u, op->ndof, op->tmp[0], s);
+    const double* dl = stage_in(lambda, op->ndof, op->tmp[1], s);
+    double* g = grow(op->tmp[6], (size_t)op->E);
     const geo_mesh* m = op->mesh;
     k_elem_gradient<<<(unsigned)cdiv(op->E, 128), 128, 0, s>>>(op->phys, m->xyz.p, m->conn.p, op->N, op->E,
                                                                op->coef.p, op->cl, op->cm, op->mask_orig.p, du, dl,
-                                                               g.p);
+                                                               g);
     check_launch(op->ctx, "k_elem_gradient");
-    copy_out(grad_e, g.p, op->E, s);
+    copy_out(grad_e, g, op->E, s);
     sync(op->ctx, "geo_op_element_gradient");
     GEO_API_END
 }
@@ -1117,15 +1129,11 @@ int geo_forward(geo_op* op, const double* f, const geo_cg_opts* opts, double* u,
     cg_opts_fill(opts, o);
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
-    DevBuf<double> tf, xo;
-    const double* df = stage_in(f, n, tf, s);
+    const double* df = stage_in(f, n, op->tmp[0], s);
     lift_new(op, df, op->bvec.p);
     const int status = solve_new(op, o, st);
     double* dst = u;
-    if (!is_device_ptr(u)) {
-        xo.alloc(n);
-        dst = xo.p;
-    }
+    if (!is_device_ptr(u)) dst = grow(op->tmp[1], (size_t)n);
     to_orig(op, op->xvec.p, dst);
     if (dst != u) copy_out(u, dst, n, s);
     sync(op->ctx, "geo_forward");
@@ -1141,23 +1149,24 @@ int geo_vjp(geo_op* op, const double* f, const double* u, const double* dJ_du, c
     cg_opts_fill(opts, o);
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
-    DevBuf<double> tu, tg, uo(n), lo(n), ge(op->E);
+    double* lo = grow(op->tmp[3], (size_t)n);
+    double* ge = grow(op->tmp[6], (size_t)op->E);
     const double* du = nullptr;
     if (u) {
-        du = stage_in(u, n, tu, s);
+        du = stage_in(u, n, op->tmp[0], s);
     } else {
         // recompute the forward solution instead of storing it
-        DevBuf<double> tf;
-        const double* df = stage_in(f, n, tf, s);
+        const double* df = stage_in(f, n, op->tmp[0], s);
         lift_new(op, df, op->bvec.p);
         const int fs = solve_new(op, o, nullptr);
         if (fs != GEO_OK) return finish_status(op->ctx, fs);
-        to_orig(op, op->xvec.p, uo.p);
-        du = uo.p;
+        double* uo = grow(op->tmp[2], (size_t)n);
+        to_orig(op, op->xvec.p, uo);
+        du = uo;
     }
     // adjoint right-hand side: dJ/du on free DOFs, zero on Dirichlet DOFs (K_bc
     // is symmetric and its Dirichlet rows are decoupled, so lambda_D = 0)
-    const double* dg = stage_in(dJ_du, n, tg, s);
+    const double* dg = stage_in(dJ_du, n, op->tmp[1], s);
     to_new(op, dg, op->bvec.p);
     k_zero_dir<double><<<nblk(n), 256, 0, s>>>(op->flags.p, op->dpn, n, op->bvec.p);
     check_launch(op->ctx, "adjoint rhs");
@@ -1166,11 +1175,11 @@ int geo_vjp(geo_op* op, const double* f, const double* u, const double* dJ_du, c
     // then O(1)) and scale lambda back, so that the absolute breakdown and
     // stopping thresholds of the CG loop do not depend on the misfit's units or
     // on the stiffness scale.
-    DevBuf<unsigned long long> mx(1);
-    GEO_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(unsigned long long), s));
-    k_max_abs_scaled<<<nblk(n), 256, 0, s>>>(op->bvec.p, op->dinv64.p, n, mx.p);
+    unsigned long long* mx = grow(op->tmpu[1], 1);
+    GEO_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned long long), s));
+    k_max_abs_scaled<<<nblk(n), 256, 0, s>>>(op->bvec.p, op->dinv64.p, n, mx);
     unsigned long long bits = 0;
-    GEO_CUDA(cudaMemcpyAsync(&bits, mx.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    GEO_CUDA(cudaMemcpyAsync(&bits, mx, sizeof(bits), cudaMemcpyDeviceToHost, s));
     sync(op->ctx, "adjoint scale");
     double zmax;
     std::memcpy(&zmax, &bits, sizeof(double));
@@ -1182,13 +1191,13 @@ int geo_vjp(geo_op* op, const double* f, const double* u, const double* dJ_du, c
     } else {
         GEO_CUDA(cudaMemsetAsync(op->xvec.p, 0, n * sizeof(double), s));
     }
-    to_orig(op, op->xvec.p, lo.p);
+    to_orig(op, op->xvec.p, lo);
     const geo_mesh* m = op->mesh;
     k_elem_gradient<<<(unsigned)cdiv(op->E, 128), 128, 0, s>>>(op->phys, m->xyz.p, m->conn.p, op->N, op->E,
                                                                op->coef.p, op->cl, op->cm, op->mask_orig.p, du,
-                                                               lo.p, ge.p);
+                                                               lo, ge);
     check_launch(op->ctx, "k_elem_gradient");
-    copy_out(dJ_dlncoef, ge.p, op->E, s);
+    copy_out(dJ_dlncoef, ge, op->E, s);
     sync(op->ctx, "geo_vjp");
     return finish_status(op->ctx, status);
     GEO_API_END
@@ -1200,8 +1209,7 @@ int geo_op_time_pcg_kernels(geo_op* op, const double* b, int32_t precision, int3
     GEO_CHECK_ARG(op && b && patch_ms && update_ms, "NULL argument");
     GEO_CHECK_ARG(iterations >= 1 && iterations <= 4096, "iterations must be in [1, 4096]");
     cudaStream_t s = op->ctx->stream;
-    DevBuf<double> tb;
-    const double* db = stage_in(b, op->ndof, tb, s);
+    const double* db = stage_in(b, op->ndof, op->tmp[0], s);
     to_new(op, db, op->bvec.p);
     time_iterations(op, precision == GEO_PRECISION_MIXED, iterations, patch_ms, update_ms);
     GEO_API_END
