@@ -97,6 +97,10 @@ _SIGS = {
     "geo_op_apply": [_P, _DP, _DP, _I32],
     "geo_op_lift_rhs": [_P, _DP, _DP],
     "geo_op_diagonal": [_P, _DP],
+    "geo_face_flux": [_P, _P, C.c_int64, _DP, _DP, _D, _DP],
+    "geo_face_area": [_P, _P, C.c_int64, _DP, _DP],
+    "geo_find_boundary_faces": [_P, _P, _DP, C.c_int64, _DP, C.POINTER(C.c_int64)],
+    "geo_apply_neumann_bcs": [_P, _P, C.c_int64, _DP, _DP, _D, C.c_int64, _DP],
     "geo_cg_solve_noalloc": [_P, _P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_cg_solve_matfree": [_P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_op_element_gradient": [_P, _DP, _DP, _DP],

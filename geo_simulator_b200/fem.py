@@ -28,7 +28,8 @@ from ._native import GeoError
 __all__ = [
     "Context", "Mesh", "ImprovedMeshGenerator", "DofManager", "IsotropicElasticity", "CsrMatrix",
     "ElementMatrix", "ElasticityElement", "BodyForce", "Assembler", "SolverStats", "ConjugateGradient",
-    "ThermalOperator", "ElasticityOperator", "GeoError",
+    "ThermalOperator", "ElasticityOperator", "GeoError", "BoundaryFace", "NeumannBC", "BoundaryConditions",
+    "Tet10Face",
 ]
 
 
@@ -440,6 +441,42 @@ class Assembler:
     assemble_elasticity_stiffness_serial = assemble_elasticity_stiffness_parallel
 
     @staticmethod
+    def find_boundary_faces(mesh: Mesh, condition, ctx=None):
+        """assembly.rs:287-309. ``condition`` is a callable on the node coordinates
+        (an [N, 3] array, vectorised) returning a boolean per node, or a boolean
+        mask itself. Returns [(element_id, local_face_id)] as an int32 [n, 2] array."""
+        ctx = _ctx(ctx)
+        mask = condition(mesh.nodes) if callable(condition) else condition
+        mask = np.ascontiguousarray(np.asarray(mask, bool).astype(np.uint8))
+        if mask.shape != (mesh.num_nodes(),):
+            raise GeoError(N.GEO_ERR_INVALID_ARG, "condition must give one value per node")
+        n = C.c_int64()
+        L = N.lib()
+        ctx.check(L.geo_find_boundary_faces(ctx.h, mesh.handle(ctx), _ptr(mask), 0, None, C.byref(n)))
+        faces = np.empty((n.value, 2), np.int32)
+        if n.value:
+            ctx.check(L.geo_find_boundary_faces(ctx.h, mesh.handle(ctx), _ptr(mask), n.value, _ptr(faces),
+                                                C.byref(n)))
+        return faces
+
+    @staticmethod
+    def apply_neumann_bcs(mesh: Mesh, f, bcs, ctx=None):
+        """assembly.rs:248-274: f[node] += face flux contributions, in place.
+        ``bcs`` is a BoundaryConditions or a (faces [n, 2], flux) pair."""
+        ctx = _ctx(ctx)
+        faces, flux = bcs.arrays() if isinstance(bcs, BoundaryConditions) else bcs
+        faces = np.ascontiguousarray(faces, np.int32).reshape(-1, 2)
+        fl = np.asarray(flux, np.float64)
+        flp = np.ascontiguousarray(np.broadcast_to(fl, (faces.shape[0],))) if fl.ndim > 0 else None
+        if not (isinstance(f, np.ndarray) and f.dtype == np.float64 and f.flags["C_CONTIGUOUS"]) and \
+                not hasattr(f, "data_ptr"):
+            raise TypeError("f must be a contiguous float64 array (updated in place)")
+        n_f = f.shape[0] if isinstance(f, np.ndarray) else f.numel()
+        ctx.check(N.lib().geo_apply_neumann_bcs(ctx.h, mesh.handle(ctx), faces.shape[0], _ptr(faces), _ptr(flp),
+                                                float(fl) if fl.ndim == 0 else 0.0, n_f, _ptr(f)))
+        return f
+
+    @staticmethod
     def assemble_gravity_load(mesh: Mesh, dof_mgr: DofManager, density, gravity, ctx=None):
         ctx = _ctx(ctx)
         g = np.ascontiguousarray(gravity, np.float64)
@@ -447,6 +484,89 @@ class Assembler:
         ctx.check(N.lib().geo_assemble_gravity_load(ctx.h, mesh.handle(ctx), dof_mgr.handle(ctx), float(density),
                                                     _ptr(g), _ptr(f)))
         return f
+
+
+# --------------------------------------------------------------------------- Neumann boundary
+@dataclass(frozen=True)
+class BoundaryFace:
+    """boundary.rs:9-15: (element, local face); local face f is opposite vertex f."""
+    element_id: int
+    local_face_id: int
+
+
+@dataclass
+class NeumannBC:
+    """boundary.rs:18-23: prescribed flux on a face."""
+    flux: float
+
+
+class BoundaryConditions:
+    """boundary.rs:26-59: the Neumann faces and their fluxes (insertion order kept)."""
+
+    def __init__(self):
+        self._neumann = {}
+
+    @staticmethod
+    def new():
+        return BoundaryConditions()
+
+    def add_neumann(self, face: BoundaryFace, flux: float):
+        self._neumann[face] = NeumannBC(float(flux))
+
+    def get_neumann(self, face: BoundaryFace):
+        return self._neumann.get(face)
+
+    def neumann_faces(self):
+        return list(self._neumann.items())
+
+    def num_neumann_bcs(self) -> int:
+        return len(self._neumann)
+
+    def arrays(self):
+        """(faces int32 [n, 2], flux float64 [n]) in insertion order."""
+        items = self.neumann_faces()
+        faces = np.array([[f.element_id, f.local_face_id] for f, _ in items], np.int32).reshape(-1, 2)
+        flux = np.array([bc.flux for _, bc in items], np.float64)
+        return faces, flux
+
+
+class Tet10Face:
+    """boundary.rs:66-267: a 6-node face of a Tet10 (3 vertices then 3 midpoints)."""
+
+    # local element node of each face node, boundary.rs:91-127
+    FACE_NODES = np.array([[1, 2, 3, 5, 9, 8], [0, 2, 3, 6, 9, 7], [0, 1, 3, 4, 8, 7], [0, 1, 2, 4, 5, 6]],
+                          np.int32)
+
+    def __init__(self, nodes):
+        self.nodes = np.asarray(nodes, np.int64)
+
+    @staticmethod
+    def from_element_face(element_nodes, local_face: int) -> "Tet10Face":
+        if not 0 <= int(local_face) <= 3:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, f"Invalid face index for tet10: {local_face}")
+        return Tet10Face(np.asarray(element_nodes)[Tet10Face.FACE_NODES[int(local_face)]])
+
+    @staticmethod
+    def integrate_flux_faces(mesh: Mesh, faces, flux, ctx=None):
+        """integrate_flux for many (element, local face) pairs on the GPU: [n, 6]."""
+        ctx = _ctx(ctx)
+        faces = np.ascontiguousarray(faces, np.int32).reshape(-1, 2)
+        fl = np.asarray(flux, np.float64)
+        per_face = fl.ndim > 0
+        flp = np.ascontiguousarray(np.broadcast_to(fl, (faces.shape[0],))) if per_face else None
+        out = np.empty((faces.shape[0], 6))
+        ctx.check(N.lib().geo_face_flux(ctx.h, mesh.handle(ctx), faces.shape[0], _ptr(faces), _ptr(flp),
+                                        float(fl) if not per_face else 0.0, _ptr(out)))
+        return out
+
+    @staticmethod
+    def area_faces(mesh: Mesh, faces, ctx=None):
+        """area for many faces on the GPU."""
+        ctx = _ctx(ctx)
+        faces = np.ascontiguousarray(faces, np.int32).reshape(-1, 2)
+        out = np.empty(faces.shape[0])
+        ctx.check(N.lib().geo_face_area(ctx.h, mesh.handle(ctx), faces.shape[0], _ptr(faces), _ptr(out)))
+        return out
 
 
 # --------------------------------------------------------------------------- solvers

@@ -161,6 +161,27 @@ int geo_assemble_elasticity_stiffness(geo_ctx* ctx, const geo_mesh* mesh, const 
 int geo_assemble_gravity_load(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs,
                               double density, const double gravity[3], double* f);
 
+/* ------------------------------------------------------------------ Neumann (flux) boundary */
+/* Faces are (element, local face) int32 pairs; local face f is the face opposite
+ * vertex f, with the 6 nodes of Tet10Face::from_element_face (boundary.rs:89-130).
+ * Per-face flux: flux_f[n_faces], or NULL for the uniform scalar flux.          */
+/* Tet10Face::integrate_flux (boundary.rs:202-266) for many faces: fe[n_faces][6] */
+int geo_face_flux(geo_ctx* ctx, const geo_mesh* mesh, int64_t n_faces, const int32_t* faces,
+                  const double* flux_f, double flux, double* fe);
+/* Tet10Face::area (boundary.rs:136-196): area[n_faces] */
+int geo_face_area(geo_ctx* ctx, const geo_mesh* mesh, int64_t n_faces, const int32_t* faces, double* area);
+/* Assembler::find_boundary_faces (assembly.rs:287-309) with the condition evaluated
+ * per node by the caller: node_mask[n_nodes] != 0 where it holds. Writes the faces
+ * whose 6 nodes all satisfy it, in (element, local face) order, and their count;
+ * faces may be NULL to query the count (capacity max_faces pairs).            */
+int geo_find_boundary_faces(geo_ctx* ctx, const geo_mesh* mesh, const uint8_t* node_mask, int64_t max_faces,
+                            int32_t* faces, int64_t* n_faces);
+/* Assembler::apply_neumann_bcs (assembly.rs:248-274): f[node] += face flux
+ * contributions (f indexed by node id, n_f >= n_nodes, updated in place). The
+ * sum per node runs in face order (deterministic).                             */
+int geo_apply_neumann_bcs(geo_ctx* ctx, const geo_mesh* mesh, int64_t n_faces, const int32_t* faces,
+                          const double* flux_f, double flux, int64_t n_f, double* f);
+
 /* sprs CsMat<f64> stand-in (device resident). */
 int geo_csr_create(geo_ctx* ctx, int64_t n_rows, int64_t n_cols, int64_t nnz, const int64_t* indptr,
                    const int32_t* indices, const double* data, geo_csr** out);

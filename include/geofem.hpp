@@ -33,6 +33,7 @@
 
 #include <array>
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -229,8 +230,63 @@ private:
     Context* ctx_ = nullptr;
 };
 
+// ---------------------------------------------------------------- Neumann boundary
+// boundary.rs:9-59: a face is (element, local face), local face f opposite vertex f
+struct BoundaryFace {
+    int32_t element_id;
+    int32_t local_face_id;
+};
+
+class BoundaryConditions {
+public:
+    void add_neumann(BoundaryFace face, double flux) {
+        faces_.push_back(face);
+        flux_.push_back(flux);
+    }
+    size_t num_neumann_bcs() const { return faces_.size(); }
+    const std::vector<BoundaryFace>& faces() const { return faces_; }
+    const std::vector<double>& fluxes() const { return flux_; }
+
+private:
+    std::vector<BoundaryFace> faces_;
+    std::vector<double> flux_;
+};
+
+struct Tet10Face {
+    std::array<int32_t, 6> nodes;  // 3 vertices then 3 edge midpoints (boundary.rs:89-130)
+    static Tet10Face from_element_face(const Tet10& element_nodes, int local_face) {
+        static const int kFace[4][6] = {{1, 2, 3, 5, 9, 8}, {0, 2, 3, 6, 9, 7}, {0, 1, 3, 4, 8, 7}, {0, 1, 2, 4, 5, 6}};
+        if (local_face < 0 || local_face > 3) throw Error(GEO_ERR_INVALID_ARG, "Invalid face index for tet10");
+        Tet10Face f;
+        for (int i = 0; i < 6; ++i) f.nodes[i] = element_nodes[kFace[local_face][i]];
+        return f;
+    }
+};
+
 // ---------------------------------------------------------------- assembly
 struct Assembler {
+    // assembly.rs:287-309: faces whose 6 nodes all satisfy the condition, in (element, face) order
+    static std::vector<BoundaryFace> find_boundary_faces(const Mesh& mesh,
+                                                         const std::function<bool(const Point3&)>& condition,
+                                                         Context& ctx = Context::default_context()) {
+        std::vector<uint8_t> mask(mesh.num_nodes());
+        for (size_t i = 0; i < mask.size(); ++i) mask[i] = condition(mesh.nodes[i]) ? 1 : 0;
+        int64_t n = 0;
+        ctx.check(geo_find_boundary_faces(ctx.get(), mesh.handle(ctx), mask.data(), 0, nullptr, &n));
+        std::vector<BoundaryFace> faces((size_t)n);
+        if (n)
+            ctx.check(geo_find_boundary_faces(ctx.get(), mesh.handle(ctx), mask.data(), n,
+                                              reinterpret_cast<int32_t*>(faces.data()), &n));
+        return faces;
+    }
+    // assembly.rs:248-274: f[node] += face flux contributions
+    static void apply_neumann_bcs(const Mesh& mesh, std::vector<double>& f, const BoundaryConditions& bcs,
+                                  Context& ctx = Context::default_context()) {
+        if (f.size() < mesh.num_nodes()) throw Error(GEO_ERR_INVALID_ARG, "f shorter than the node count");
+        ctx.check(geo_apply_neumann_bcs(ctx.get(), mesh.handle(ctx), (int64_t)bcs.num_neumann_bcs(),
+                                        reinterpret_cast<const int32_t*>(bcs.faces().data()), bcs.fluxes().data(),
+                                        0.0, (int64_t)f.size(), f.data()));
+    }
     // assembly.rs:69-117 (uniform conductivity) and the per-element variant
     static CsMat assemble_thermal_stiffness_parallel(const Mesh& mesh, const DofManager& dofs, double conductivity,
                                                      Context& ctx = Context::default_context()) {

@@ -959,3 +959,108 @@ void orc_elasticity_element_gradient(int64_t n_nodes, const double* xyz, int64_t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- Neumann (flux) boundary
+// Tet10Face::from_element_face, fem/boundary.rs:89-130: 3 vertices then the 3
+// edge midpoints of local face f (face f is opposite vertex f).
+static const int kFace[4][6] = {
+    {1, 2, 3, 5, 9, 8},
+    {0, 2, 3, 6, 9, 7},
+    {0, 1, 3, 4, 8, 7},
+    {0, 1, 2, 4, 5, 6},
+};
+
+void orc_face_nodes(const int64_t elem[10], int local_face, int64_t out[6]) {
+    for (int i = 0; i < 6; ++i) out[i] = elem[kFace[local_face][i]];
+}
+
+// 6-node triangle shape functions and derivatives in area coordinates (L1, L2),
+// L3 = 1 - L1 - L2, boundary.rs:145-167 / :206-228.
+static void tri6(double l1, double l2, double N[6], double d[6][2]) {
+    const double l3 = 1.0 - l1 - l2;
+    N[0] = l1 * (2.0 * l1 - 1.0);
+    N[1] = l2 * (2.0 * l2 - 1.0);
+    N[2] = l3 * (2.0 * l3 - 1.0);
+    N[3] = 4.0 * l1 * l2;
+    N[4] = 4.0 * l2 * l3;
+    N[5] = 4.0 * l3 * l1;
+    d[0][0] = 4.0 * l1 - 1.0;  d[0][1] = 0.0;
+    d[1][0] = 0.0;             d[1][1] = 4.0 * l2 - 1.0;
+    d[2][0] = -4.0 * l3 + 1.0; d[2][1] = -4.0 * l3 + 1.0;
+    d[3][0] = 4.0 * l2;        d[3][1] = 4.0 * l1;
+    d[4][0] = -4.0 * l2;       d[4][1] = 4.0 * (l3 - l2);
+    d[5][0] = 4.0 * (l3 - l1); d[5][1] = -4.0 * l1;
+}
+
+// 3-point triangle rule, boundary.rs:172-176 / :232-236 (weights sum to 1/2)
+static const double kTriQ[3][3] = {
+    {1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0},
+    {2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0},
+    {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0},
+};
+
+// |dx/dL1 x dx/dL2| at (l1, l2); coords [6][3]
+static double tri6_detj(const double* c, const double d[6][2]) {
+    double a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+    for (int i = 0; i < 6; ++i)
+        for (int k = 0; k < 3; ++k) {
+            a[k] += c[3 * i + k] * d[i][0];
+            b[k] += c[3 * i + k] * d[i][1];
+        }
+    const double x = a[1] * b[2] - a[2] * b[1], y = a[2] * b[0] - a[0] * b[2], z = a[0] * b[1] - a[1] * b[0];
+    return std::sqrt(x * x + y * y + z * z);
+}
+
+// Tet10Face::area, boundary.rs:136-196
+double orc_face_area(const double coords[18]) {
+    double area = 0.0;
+    for (int q = 0; q < 3; ++q) {
+        double N[6], d[6][2];
+        tri6(kTriQ[q][0], kTriQ[q][1], N, d);
+        area += kTriQ[q][2] * tri6_detj(coords, d);
+    }
+    return area;
+}
+
+// Tet10Face::integrate_flux, boundary.rs:202-266: f_i = sum_q w_q N_i flux |det J|
+void orc_face_flux(const double coords[18], double flux, double f[6]) {
+    for (int i = 0; i < 6; ++i) f[i] = 0.0;
+    for (int q = 0; q < 3; ++q) {
+        double N[6], d[6][2];
+        tri6(kTriQ[q][0], kTriQ[q][1], N, d);
+        const double dj = tri6_detj(coords, d);
+        for (int i = 0; i < 6; ++i) f[i] += kTriQ[q][2] * N[i] * flux * dj;
+    }
+}
+
+// Assembler::find_boundary_faces, assembly.rs:287-309: faces whose 6 nodes all
+// satisfy the condition (node_mask), element-major then local face. Returns the count.
+int64_t orc_find_boundary_faces(int64_t n_elem, const int64_t* conn, const uint8_t* node_mask, int64_t* faces) {
+    int64_t n = 0;
+    for (int64_t e = 0; e < n_elem; ++e)
+        for (int f = 0; f < 4; ++f) {
+            bool all = true;
+            for (int i = 0; i < 6 && all; ++i) all = node_mask[conn[10 * e + kFace[f][i]]] != 0;
+            if (all) {
+                faces[2 * n] = e;
+                faces[2 * n + 1] = f;
+                ++n;
+            }
+        }
+    return n;
+}
+
+// Assembler::apply_neumann_bcs, assembly.rs:248-274: f[node] += face flux
+// contributions, faces in the given order.
+void orc_apply_neumann_bcs(const double* xyz, const int64_t* conn, int64_t n_faces, const int64_t* faces,
+                           const double* flux, double* f) {
+    for (int64_t k = 0; k < n_faces; ++k) {
+        int64_t nodes[6];
+        orc_face_nodes(conn + 10 * faces[2 * k], (int)faces[2 * k + 1], nodes);
+        double c[18], fe[6];
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 3; ++j) c[3 * i + j] = xyz[3 * nodes[i] + j];
+        orc_face_flux(c, flux[k], fe);
+        for (int i = 0; i < 6; ++i) f[nodes[i]] += fe[i];
+    }
+}

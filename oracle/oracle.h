@@ -109,6 +109,14 @@ void orc_elasticity_element_gradient(int64_t n_nodes, const double* xyz, int64_t
                                      const int64_t* conn, const double* E_e, double nu,
                                      const double* u, const double* lam, double* g);
 
+/* ---- Neumann boundary: fem/boundary.rs:89-266, assembly.rs:248-309 ---- */
+void orc_face_nodes(const int64_t elem[10], int local_face, int64_t out[6]);
+double orc_face_area(const double coords[18]);
+void orc_face_flux(const double coords[18], double flux, double f[6]);
+int64_t orc_find_boundary_faces(int64_t n_elem, const int64_t* conn, const uint8_t* node_mask, int64_t* faces);
+void orc_apply_neumann_bcs(const double* xyz, const int64_t* conn, int64_t n_faces, const int64_t* faces,
+                           const double* flux, double* f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,11 @@ def _declare(L):
         "orc_thermal_element_gradient": (None, [C.c_int64, _D, C.c_int64, _I64, _D, _D, _D, _D]),
         "orc_elasticity_element_gradient": (None, [C.c_int64, _D, C.c_int64, _I64, _D, C.c_double,
                                                    _D, _D, _D]),
+        "orc_face_nodes": (None, [_I64, C.c_int, _I64]),
+        "orc_face_area": (C.c_double, [_D]),
+        "orc_face_flux": (None, [_D, C.c_double, _D]),
+        "orc_find_boundary_faces": (C.c_int64, [C.c_int64, _I64, _U8, _I64]),
+        "orc_apply_neumann_bcs": (None, [_D, _I64, C.c_int64, _I64, _D, _D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -422,6 +427,43 @@ def elasticity_element_gradient(xyz, conn, E_e, nu, u, lam):
                                           _d(_f64(E_e)), float(nu), _d(_f64(u)), _d(_f64(lam)),
                                           _d(g))
     return g
+
+
+# ------------------------------------------------------------------- Neumann boundary
+def face_nodes(elem, local_face):
+    """Tet10Face::from_element_face (boundary.rs:89-130)."""
+    out = np.empty(6, np.int64)
+    lib().orc_face_nodes(_i(_i64(elem)), int(local_face), _i(out))
+    return out
+
+
+def face_area(coords6):
+    return lib().orc_face_area(_d(_f64(coords6)))
+
+
+def face_flux(coords6, flux):
+    """Tet10Face::integrate_flux (boundary.rs:202-266)."""
+    f = np.empty(6)
+    lib().orc_face_flux(_d(_f64(coords6)), float(flux), _d(f))
+    return f
+
+
+def find_boundary_faces(conn, node_mask):
+    """Assembler::find_boundary_faces (assembly.rs:287-309) with the condition
+    evaluated per node: [(element, local_face)] whose 6 nodes all satisfy it."""
+    conn = _i64(conn)
+    faces = np.empty((4 * conn.shape[0], 2), np.int64)
+    n = lib().orc_find_boundary_faces(conn.shape[0], _i(conn), np.ascontiguousarray(node_mask, np.uint8).ctypes.data_as(_U8), _i(faces))
+    return faces[:n].copy()
+
+
+def apply_neumann_bcs(xyz, conn, faces, flux, f):
+    """Assembler::apply_neumann_bcs (assembly.rs:248-274); returns f + face fluxes."""
+    xyz, conn, faces = _f64(xyz), _i64(conn), _i64(faces).reshape(-1, 2)
+    flux = np.broadcast_to(np.asarray(flux, np.float64), (faces.shape[0],)).copy()
+    out = _f64(f).copy()
+    lib().orc_apply_neumann_bcs(_d(xyz), _i(conn), faces.shape[0], _i(faces), _d(flux), _d(out))
+    return out
 
 
 # ------------------------------------------------------------------- problem setups

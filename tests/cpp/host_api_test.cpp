@@ -90,6 +90,34 @@ void thermal_profile() {
     }
 }
 
+// -k T'' = Q, T(0) = T0, k T'(L) = q: Neumann flux on the top face (apply_neumann_bcs)
+void flux_profile() {
+    const double lz = 600, k = 3.0, Q = 1e-6, T0 = 1280, q = 0.02;
+    Mesh mesh = ImprovedMeshGenerator::generate_cube(4, 4, 4, 1000, 1000, lz);
+    DofManager dofs(mesh.num_nodes(), 1);
+    for (size_t i = 0; i < mesh.num_nodes(); ++i)
+        if (std::fabs(mesh.nodes[i][2]) < 1.0) dofs.set_dirichlet_node(i, T0);
+    CsMat K = Assembler::assemble_thermal_stiffness_parallel(mesh, dofs, k);
+    std::vector<double> f = Assembler::assemble_thermal_load(mesh, dofs, Q);
+    BoundaryConditions bcs;
+    for (const BoundaryFace& face :
+         Assembler::find_boundary_faces(mesh, [&](const Point3& p) { return std::fabs(p[2] - lz) < 1.0; }))
+        bcs.add_neumann(face, q);
+    Assembler::apply_neumann_bcs(mesh, f, bcs);
+    auto kb = Assembler::apply_dirichlet_bcs(K, f, dofs);
+    auto sol = ConjugateGradient().with_max_iterations(2000).with_tolerance(1e-12).solve(kb.first, kb.second);
+    double err = 0, scale = 0;
+    for (size_t i = 0; i < mesh.num_nodes(); ++i) {
+        const double z = mesh.nodes[i][2];
+        const double exact = T0 + (Q * lz + q) * z / k - Q * z * z / (2 * k);
+        err = std::fmax(err, std::fabs(sol.first[i] - exact));
+        scale = std::fmax(scale, std::fabs(exact));
+    }
+    expect(sol.second.converged && bcs.num_neumann_bcs() == 32 && err <= 1e-6 * scale,
+           "Neumann flux profile 4^3: max error " + sci(err) + " (" + std::to_string(bcs.num_neumann_bcs()) +
+               " top faces)");
+}
+
 void small_cg() {
     CsMat A = CsMat::from_arrays(2, 2, {0, 2, 4}, {0, 1, 0, 1}, {2.0, 1.0, 1.0, 2.0});
     auto s = ConjugateGradient().solve(A, {3.0, 3.0});
@@ -230,6 +258,7 @@ int main() {
         small_cg();
         thermal_profile();
         patch_test();
+        flux_profile();
         errors();
         adjoint_fd();
     } catch (const Error& e) {
