@@ -9,7 +9,8 @@ of ``include/geo_fem.h`` (``libgeofem.so``).
 from .fem import (  # noqa: F401
     Assembler, BodyForce, BoundaryConditions, BoundaryFace, ConjugateGradient, Context, CsrMatrix, DofManager,
     ElasticityElement, ElasticityOperator, ElementMatrix, GeoError, ImprovedMeshGenerator, IsotropicElasticity,
-    Mesh, NeumannBC, SolverStats, Tet10Face, ThermalOperator,
+    MaxwellViscoelasticity, Mesh, NeumannBC, SolverStats, StressHistory, Tet10Face, ThermalOperator, BackwardEuler,
+    TimeStepStats, update_stresses_maxwell,
 )
 
 __version__ = "0.1.0"

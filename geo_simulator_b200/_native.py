@@ -101,6 +101,9 @@ _SIGS = {
     "geo_face_area": [_P, _P, C.c_int64, _DP, _DP],
     "geo_find_boundary_faces": [_P, _P, _DP, C.c_int64, _DP, C.POINTER(C.c_int64)],
     "geo_apply_neumann_bcs": [_P, _P, C.c_int64, _DP, _DP, _D, C.c_int64, _DP],
+    "geo_maxwell_history_force": [_P, _P, _DP, _DP],
+    "geo_assemble_maxwell_viscoelastic": [_P, _P, _P, _D, _D, _D, _D, _DP, C.POINTER(C.c_void_p), _DP],
+    "geo_update_stresses_maxwell": [_P, _P, _D, _D, _D, _DP, _DP, _D, _DP, _DP],
     "geo_cg_solve_noalloc": [_P, _P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_cg_solve_matfree": [_P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_op_element_gradient": [_P, _DP, _DP, _DP],

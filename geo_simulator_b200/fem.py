@@ -29,7 +29,8 @@ __all__ = [
     "Context", "Mesh", "ImprovedMeshGenerator", "DofManager", "IsotropicElasticity", "CsrMatrix",
     "ElementMatrix", "ElasticityElement", "BodyForce", "Assembler", "SolverStats", "ConjugateGradient",
     "ThermalOperator", "ElasticityOperator", "GeoError", "BoundaryFace", "NeumannBC", "BoundaryConditions",
-    "Tet10Face",
+    "Tet10Face", "MaxwellViscoelasticity", "StressHistory", "BackwardEuler", "TimeStepStats",
+    "update_stresses_maxwell",
 ]
 
 
@@ -112,6 +113,7 @@ class Mesh:
             raise GeoError(N.GEO_ERR_INVALID_ARG, "element references a node id out of range")
         self.elements = np.ascontiguousarray(el, dtype=np.int32).reshape(-1, 10)
         self._handles = {}
+        self.stress_history = None  # StressHistory for viscoelasticity (mesh/geometry.rs)
 
     def num_nodes(self) -> int:
         return int(self.nodes.shape[0])
@@ -149,7 +151,7 @@ class ImprovedMeshGenerator:
         conn = np.empty((n_elem.value, 10), np.int32)
         N.check(L.geo_generate_cube(nx, ny, nz, float(lx), float(ly), float(lz), _ptr(xyz), _ptr(conn)))
         m = Mesh.__new__(Mesh)
-        m.nodes, m.elements, m._handles = xyz, conn, {}
+        m.nodes, m.elements, m._handles, m.stress_history = xyz, conn, {}, None
         return m
 
 
@@ -477,6 +479,31 @@ class Assembler:
         return f
 
     @staticmethod
+    def maxwell_history_force(mesh: Mesh, stress_history, ctx=None):
+        """f_history of assemble_maxwell_viscoelastic_parallel (assembly.rs:959-1020)."""
+        ctx = _ctx(ctx)
+        st = stress_history.stress if isinstance(stress_history, StressHistory) else stress_history
+        st = np.ascontiguousarray(st, np.float64)
+        f = np.empty(3 * mesh.num_nodes())
+        ctx.check(N.lib().geo_maxwell_history_force(ctx.h, mesh.handle(ctx), _ptr(st), _ptr(f)))
+        return f
+
+    @staticmethod
+    def assemble_maxwell_viscoelastic_parallel(mesh: Mesh, dof_mgr: DofManager, material, dt, ctx=None):
+        """assembly.rs:959-1020: (elastic K, f_history) from mesh.stress_history."""
+        ctx = _ctx(ctx)
+        if mesh.stress_history is None:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, "Mesh must have stress_history for viscoelasticity")
+        st = np.ascontiguousarray(mesh.stress_history.stress, np.float64)
+        h = C.c_void_p()
+        f = np.empty(dof_mgr.total_dofs())
+        ctx.check(N.lib().geo_assemble_maxwell_viscoelastic(ctx.h, mesh.handle(ctx), dof_mgr.handle(ctx),
+                                                            material.youngs_modulus, material.poisson_ratio,
+                                                            material.viscosity, float(dt), _ptr(st), C.byref(h),
+                                                            _ptr(f)))
+        return CsrMatrix(h, ctx), f
+
+    @staticmethod
     def assemble_gravity_load(mesh: Mesh, dof_mgr: DofManager, density, gravity, ctx=None):
         ctx = _ctx(ctx)
         g = np.ascontiguousarray(gravity, np.float64)
@@ -567,6 +594,145 @@ class Tet10Face:
         out = np.empty(faces.shape[0])
         ctx.check(N.lib().geo_face_area(ctx.h, mesh.handle(ctx), faces.shape[0], _ptr(faces), _ptr(out)))
         return out
+
+
+# --------------------------------------------------------------------------- Maxwell viscoelasticity
+@dataclass
+class MaxwellViscoelasticity:
+    """mechanics/constitutive.rs:286-395: E (Pa), nu, viscosity mu (Pa s)."""
+    youngs_modulus: float
+    poisson_ratio: float
+    viscosity: float
+
+    def __post_init__(self):
+        if not self.youngs_modulus > 0:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, f"Young's modulus must be positive, got {self.youngs_modulus}")
+        if not -1.0 < self.poisson_ratio < 0.5:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, f"Poisson's ratio must be in (-1, 0.5), got {self.poisson_ratio}")
+        if not self.viscosity > 0:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, f"Viscosity must be positive, got {self.viscosity}")
+
+    @staticmethod
+    def new(youngs_modulus, poisson_ratio, viscosity):
+        return MaxwellViscoelasticity(float(youngs_modulus), float(poisson_ratio), float(viscosity))
+
+    def shear_modulus(self) -> float:
+        return self.youngs_modulus / (2.0 * (1.0 + self.poisson_ratio))
+
+    def relaxation_time(self) -> float:
+        return self.viscosity / self.shear_modulus()
+
+    def elastic_matrix(self):
+        """IsotropicElasticity::constitutive_matrix (Voigt, engineering shear)."""
+        E, nu = self.youngs_modulus, self.poisson_ratio
+        f = E / ((1.0 + nu) * (1.0 - 2.0 * nu))
+        D = np.zeros((6, 6))
+        D[:3, :3] = nu
+        np.fill_diagonal(D[:3, :3], 1.0 - nu)
+        D[3, 3] = D[4, 4] = D[5, 5] = (1.0 - 2.0 * nu) / 2.0
+        return f * D
+
+    def effective_constitutive_matrix(self, dt):
+        """D_elastic / (1 + dt / tau_M)."""
+        return self.elastic_matrix() / (1.0 + dt / self.relaxation_time())
+
+
+class StressHistory:
+    """mesh/state.rs:12-75: Voigt stress [xx yy zz xy yz zx] per element."""
+
+    def __init__(self, n_elements: int):
+        self.stress = np.zeros((int(n_elements), 6))
+
+    @staticmethod
+    def new(n_elements):
+        return StressHistory(n_elements)
+
+    def get(self, elem_id):
+        return self.stress[elem_id]
+
+    def set(self, elem_id, stress):
+        self.stress[elem_id] = stress
+
+    def update_all(self, new_stresses):
+        self.stress = np.ascontiguousarray(new_stresses, np.float64).reshape(-1, 6)
+
+    def num_elements(self):
+        return self.stress.shape[0]
+
+
+def update_stresses_maxwell(mesh: Mesh, dof_mgr: DofManager, material: MaxwellViscoelasticity, u_n, u_next, dt,
+                            ctx=None):
+    """mechanics/stress_update.rs:39-143: new [E, 6] stresses from mesh.stress_history."""
+    ctx = _ctx(ctx)
+    if mesh.stress_history is None:
+        raise GeoError(N.GEO_ERR_INVALID_ARG, "Mesh must have stress_history")
+    out = np.empty((mesh.num_elements(), 6))
+    sn = np.ascontiguousarray(mesh.stress_history.stress, np.float64)
+    ctx.check(N.lib().geo_update_stresses_maxwell(ctx.h, mesh.handle(ctx), material.youngs_modulus,
+                                                  material.poisson_ratio, material.viscosity, _ptr(_f64(u_n)),
+                                                  _ptr(_f64(u_next)), float(dt), _ptr(sn), _ptr(out)))
+    return out
+
+
+@dataclass
+class TimeStepStats:
+    """time_integration.rs:11-20."""
+    time: float
+    dt: float
+    iterations: int
+    residual: float
+
+
+class BackwardEuler:
+    """time_integration.rs:38-160: backward Euler for Maxwell viscoelasticity.
+
+    ``step`` follows the reference (assemble K_eff and f_history, add f_ext, apply
+    the Dirichlet BCs, solve). ``step_operator`` takes the same step with a
+    resident matrix-free ElasticityOperator (the elastic K does not change between
+    steps), so nothing is re-assembled."""
+
+    def __init__(self, n_dofs: int, dt: float):
+        if not dt > 0:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, f"Time step must be positive, got {dt}")
+        if not n_dofs > 0:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, f"Number of DOFs must be positive, got {n_dofs}")
+        self.time, self.dt = 0.0, float(dt)
+        self.displacement = np.zeros(int(n_dofs))
+
+    @staticmethod
+    def new(n_dofs, dt):
+        return BackwardEuler(n_dofs, dt)
+
+    def step(self, mesh: Mesh, dof_mgr: DofManager, material: MaxwellViscoelasticity, f_ext, solver):
+        K, f_hist = Assembler.assemble_maxwell_viscoelastic_parallel(mesh, dof_mgr, material, self.dt)
+        Kb, fb = Assembler.apply_dirichlet_bcs(K, np.asarray(f_ext, np.float64) + f_hist, dof_mgr)
+        u, st = solver.solve(Kb, fb)
+        return self._advance(u, st)
+
+    def step_operator(self, op: "ElasticityOperator", mesh: Mesh, f_ext, solver):
+        f_hist = Assembler.maxwell_history_force(mesh, mesh.stress_history, op.ctx)
+        u, st = op.forward(np.asarray(f_ext, np.float64) + f_hist, solver)
+        return self._advance(u, st)
+
+    def _advance(self, u, st):
+        self.displacement = u
+        self.time += self.dt
+        return u, TimeStepStats(self.time, self.dt, st.iterations, st.residual_norm)
+
+    def current_time(self):
+        return self.time
+
+    def current_displacement(self):
+        return self.displacement
+
+    def reset(self):
+        self.time = 0.0
+        self.displacement = np.zeros_like(self.displacement)
+
+    def set_timestep(self, dt):
+        if not dt > 0:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, f"Time step must be positive, got {dt}")
+        self.dt = float(dt)
 
 
 # --------------------------------------------------------------------------- solvers

@@ -182,6 +182,25 @@ int geo_find_boundary_faces(geo_ctx* ctx, const geo_mesh* mesh, const uint8_t* n
 int geo_apply_neumann_bcs(geo_ctx* ctx, const geo_mesh* mesh, int64_t n_faces, const int32_t* faces,
                           const double* flux_f, double flux, int64_t n_f, double* f);
 
+/* ------------------------------------------------------------------ Maxwell viscoelasticity */
+/* Element stresses are Voigt 6-vectors [xx yy zz xy yz zx] per element (StressHistory,
+ * mesh/state.rs:12-75), stress[n_elem][6]. Material: E > 0, nu in (-1, 0.5), mu > 0
+ * (MaxwellViscoelasticity::new, mechanics/constitutive.rs:317-329).               */
+/* The history force of assemble_maxwell_viscoelastic_parallel (assembly.rs:959-1020):
+ * f[3 n_nodes] = -sum_e sum_q w |det J| B^T sigma_e (mechanics/element.rs:257-296). */
+int geo_maxwell_history_force(geo_ctx* ctx, const geo_mesh* mesh, const double* stress, double* f);
+/* Assembler::assemble_maxwell_viscoelastic_parallel (assembly.rs:959-1020): the elastic
+ * stiffness (as geo_assemble_elasticity_stiffness with E, nu) and the history force. */
+int geo_assemble_maxwell_viscoelastic(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, double E,
+                                      double nu, double mu, double dt, const double* stress, geo_csr** K,
+                                      double* f_history);
+/* update_stresses_maxwell (mechanics/stress_update.rs:39-143): stress_next[n_elem][6]
+ * from the strain increment of u_next - u_n averaged over the 4 points, elastic
+ * predictor, deviatoric part relaxed by 1 / (1 + dt / tau_M).                    */
+int geo_update_stresses_maxwell(geo_ctx* ctx, const geo_mesh* mesh, double E, double nu, double mu,
+                                const double* u_n, const double* u_next, double dt, const double* stress_n,
+                                double* stress_next);
+
 /* sprs CsMat<f64> stand-in (device resident). */
 int geo_csr_create(geo_ctx* ctx, int64_t n_rows, int64_t n_cols, int64_t nnz, const int64_t* indptr,
                    const int32_t* indices, const double* data, geo_csr** out);

@@ -1064,3 +1064,84 @@ void orc_apply_neumann_bcs(const double* xyz, const int64_t* conn, int64_t n_fac
         for (int i = 0; i < 6; ++i) f[nodes[i]] += fe[i];
     }
 }
+
+// ---------------------------------------------------------------- Maxwell viscoelasticity
+// ElasticityElement::maxwell_viscoelastic (mechanics/element.rs:257-296), history part:
+// f_e = -sum_q w_q |det J_q| B_q^T sigma_n (4-point rule, isoparametric B); the
+// stiffness part is the elastic K_e (elasticity_stiffness). Scattered as in
+// Assembler::assemble_maxwell_viscoelastic_parallel (assembly.rs:959-1020):
+// element order, node i, component c.
+int orc_maxwell_history_force(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn,
+                              const double* stress, double* f) {
+    for (int64_t i = 0; i < 3 * n_nodes; ++i) f[i] = 0.0;
+    const Rule q = rule_4();
+    for (int64_t e = 0; e < n_elem; ++e) {
+        double nodes[30], fe[30] = {0};
+        gather_nodes(xyz, conn, e, nodes);
+        const double* sg = stress + 6 * e;
+        for (size_t p = 0; p < q.pts.size(); ++p) {
+            double J[9], dNdx[30], B[180];
+            jacobian(q.pts[p].data(), nodes, J);
+            const double w = q.w[p] * std::fabs(det3(J));
+            if (!shape_derivs_cart(q.pts[p].data(), nodes, dNdx)) return 1;
+            b_matrix(dNdx, B);
+            for (int c = 0; c < 30; ++c) {
+                double s = 0.0;
+                for (int k = 0; k < 6; ++k) s += B[30 * k + c] * sg[k];
+                fe[c] -= w * s;
+            }
+        }
+        for (int i = 0; i < 10; ++i)
+            for (int c = 0; c < 3; ++c) f[3 * conn[10 * e + i] + c] += fe[3 * i + c];
+    }
+    return 0;
+}
+
+// update_stresses_maxwell (mechanics/stress_update.rs:39-143): strain increment
+// averaged over the 4 points, elastic predictor with lambda = K - 2G/3,
+// deviatoric part relaxed by 1 / (1 + dt / tau_M), tau_M = mu / G.
+int orc_update_stresses_maxwell(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn, double E,
+                                double nu, double mu, const double* u_n, const double* u_next, double dt,
+                                const double* stress_n, double* stress_next) {
+    (void)n_nodes;
+    const double G = E / (2.0 * (1.0 + nu));
+    const double tau = mu / G;
+    const double factor = 1.0 / (1.0 + dt / tau);
+    const double Kb = E / (3.0 * (1.0 - 2.0 * nu));
+    const double lam = Kb - 2.0 * G / 3.0;
+    const Rule q = rule_4();
+    for (int64_t e = 0; e < n_elem; ++e) {
+        double nodes[30], du[30], de[6] = {0, 0, 0, 0, 0, 0};
+        gather_nodes(xyz, conn, e, nodes);
+        for (int i = 0; i < 10; ++i)
+            for (int c = 0; c < 3; ++c) {
+                const int64_t g = 3 * conn[10 * e + i] + c;
+                du[3 * i + c] = u_next[g] - u_n[g];
+            }
+        for (size_t p = 0; p < q.pts.size(); ++p) {
+            double dNdx[30], B[180];
+            if (!shape_derivs_cart(q.pts[p].data(), nodes, dNdx)) return 1;
+            b_matrix(dNdx, B);
+            for (int k = 0; k < 6; ++k) {
+                double s = 0.0;
+                for (int c = 0; c < 30; ++c) s += B[30 * k + c] * du[c];
+                de[k] += s;
+            }
+        }
+        for (int k = 0; k < 6; ++k) de[k] /= (double)q.pts.size();
+        const double* sn = stress_n + 6 * e;
+        const double tr = de[0] + de[1] + de[2];
+        double st[6] = {sn[0] + lam * tr + 2.0 * G * de[0], sn[1] + lam * tr + 2.0 * G * de[1],
+                        sn[2] + lam * tr + 2.0 * G * de[2], sn[3] + G * de[3],
+                        sn[4] + G * de[4],                  sn[5] + G * de[5]};
+        const double p = (st[0] + st[1] + st[2]) / 3.0;
+        double* o = stress_next + 6 * e;
+        o[0] = (st[0] - p) * factor + p;
+        o[1] = (st[1] - p) * factor + p;
+        o[2] = (st[2] - p) * factor + p;
+        o[3] = st[3] * factor;
+        o[4] = st[4] * factor;
+        o[5] = st[5] * factor;
+    }
+    return 0;
+}

@@ -117,6 +117,14 @@ int64_t orc_find_boundary_faces(int64_t n_elem, const int64_t* conn, const uint8
 void orc_apply_neumann_bcs(const double* xyz, const int64_t* conn, int64_t n_faces, const int64_t* faces,
                            const double* flux, double* f);
 
+/* ---- Maxwell viscoelasticity: mechanics/element.rs:257-296, assembly.rs:959-1020,
+ *      mechanics/stress_update.rs:39-143 ---- */
+int orc_maxwell_history_force(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn,
+                              const double* stress, double* f);
+int orc_update_stresses_maxwell(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn, double E,
+                                double nu, double mu, const double* u_n, const double* u_next, double dt,
+                                const double* stress_n, double* stress_next);
+
 #ifdef __cplusplus
 }
 #endif

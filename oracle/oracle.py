@@ -100,6 +100,9 @@ def _declare(L):
         "orc_face_flux": (None, [_D, C.c_double, _D]),
         "orc_find_boundary_faces": (C.c_int64, [C.c_int64, _I64, _U8, _I64]),
         "orc_apply_neumann_bcs": (None, [_D, _I64, C.c_int64, _I64, _D, _D]),
+        "orc_maxwell_history_force": (C.c_int, [C.c_int64, _D, C.c_int64, _I64, _D, _D]),
+        "orc_update_stresses_maxwell": (C.c_int, [C.c_int64, _D, C.c_int64, _I64, C.c_double, C.c_double,
+                                                  C.c_double, _D, _D, C.c_double, _D, _D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -463,6 +466,26 @@ def apply_neumann_bcs(xyz, conn, faces, flux, f):
     flux = np.broadcast_to(np.asarray(flux, np.float64), (faces.shape[0],)).copy()
     out = _f64(f).copy()
     lib().orc_apply_neumann_bcs(_d(xyz), _i(conn), faces.shape[0], _i(faces), _d(flux), _d(out))
+    return out
+
+
+# ------------------------------------------------------------------- Maxwell viscoelasticity
+def maxwell_history_force(xyz, conn, stress):
+    """f_history of assemble_maxwell_viscoelastic_parallel (assembly.rs:959-1020)."""
+    xyz, conn = _f64(xyz), _i64(conn)
+    f = np.empty(3 * xyz.shape[0])
+    assert lib().orc_maxwell_history_force(xyz.shape[0], _d(xyz), conn.shape[0], _i(conn),
+                                           _d(_f64(stress)), _d(f)) == 0
+    return f
+
+
+def update_stresses_maxwell(xyz, conn, E, nu, mu, u_n, u_next, dt, stress_n):
+    """update_stresses_maxwell (mechanics/stress_update.rs:39-143): [E, 6]."""
+    xyz, conn = _f64(xyz), _i64(conn)
+    out = np.empty((conn.shape[0], 6))
+    assert lib().orc_update_stresses_maxwell(xyz.shape[0], _d(xyz), conn.shape[0], _i(conn), float(E), float(nu),
+                                             float(mu), _d(_f64(u_n)), _d(_f64(u_next)), float(dt),
+                                             _d(_f64(stress_n)), _d(out)) == 0
     return out
 
 
