@@ -265,6 +265,8 @@ def run_ours(args, ws, rank, local, pg):
         extras.update(adjoint_ratio(ctx, args))
         extras["csr_vs_matfree_64"] = csr_vs_matfree(ctx)
         extras["elasticity_48x48x24"] = elasticity_config(ctx)
+        extras["neumann_128"] = neumann_timing(ctx, mesh)
+        extras["maxwell_step_48x48x24"] = maxwell_step(ctx)
 
     # dominant kernel: the FP32 patch kernel in PCG mode, timed launch by launch with
     # CUDA events on the context stream right after the timed region
@@ -489,6 +491,71 @@ def elasticity_config(ctx):
             "fp64_iterations": s64.iterations, "mixed_speedup_vs_fp64": t64 / tf,
             "mixed_vs_fp64_rel_l2": float(np.linalg.norm(u - u64) / np.linalg.norm(u64)),
             "adjoint_s": ta, "adjoint_forward_ratio": ta / tf, "adjoint_converged": bool(sa.converged)}
+
+
+def neumann_timing(ctx, mesh):
+    """Neumann flux on the top face of the 128^3 cube: GPU boundary-face detection
+    (find_boundary_faces) and the deterministic apply_neumann_bcs, host-timed."""
+    import geo_simulator_b200 as geo
+    top = np.abs(mesh.nodes[:, 2] - LZ) < 1.0
+    f = np.zeros(mesh.num_nodes())
+    geo.Assembler.find_boundary_faces(mesh, top, ctx)
+    t0 = time.perf_counter()
+    faces = geo.Assembler.find_boundary_faces(mesh, top, ctx)
+    t1 = time.perf_counter()
+    geo.Assembler.apply_neumann_bcs(mesh, f, (faces, 0.05), ctx)
+    t2 = time.perf_counter()
+    return {"faces": int(faces.shape[0]), "find_boundary_faces_s": t1 - t0, "apply_neumann_s": t2 - t1,
+            "total_flux": float(f.sum()), "expected_total_flux": 0.05 * LX * LY}
+
+
+def maxwell_step(ctx):
+    """One backward-Euler step of Maxwell viscoelasticity on the 48x48x24 half-space
+    (gravity, fixed base, roller sides, E = 1e11, nu = 0.25, mu = 1e19, dt = tau/10):
+    the reference's step (re-assemble K and f_history, CSR Jacobi-PCG, FP64) and the
+    step with a resident matrix-free operator (mixed precision), both followed by the
+    stress update. Rel-res 1e-8."""
+    import geo_simulator_b200 as geo
+    lx, ly, lz = 100e3, 100e3, 50e3
+    mesh = geo.ImprovedMeshGenerator.generate_cube(48, 48, 24, lx, ly, lz)
+    N = mesh.num_nodes()
+    x, y, z = mesh.nodes[:, 0], mesh.nodes[:, 1], mesh.nodes[:, 2]
+    mask = np.zeros(3 * N, np.uint8)
+    base = np.nonzero(np.abs(z) < 1.0)[0]
+    for c in range(3):
+        mask[3 * base + c] = 1
+    mask[3 * np.nonzero((np.abs(x) < 1.0) | (np.abs(x - lx) < 1.0))[0]] = 1
+    mask[3 * np.nonzero((np.abs(y) < 1.0) | (np.abs(y - ly) < 1.0))[0] + 1] = 1
+    dm = geo.DofManager(N, 3)
+    idx = np.nonzero(mask)[0]
+    dm.set_dirichlet(idx, np.zeros(idx.size))
+    mat = geo.MaxwellViscoelasticity.new(1e11, 0.25, 1e19)
+    dt = 0.1 * mat.relaxation_time()
+    f_ext = geo.Assembler.assemble_gravity_load(mesh, dm, 3300.0, [0.0, 0.0, -9.81], ctx)
+    mesh.stress_history = geo.StressHistory(mesh.num_elements())
+    mesh.stress_history.update_all(np.random.default_rng(3001).normal(0, 1e6, (mesh.num_elements(), 6)))
+    csr_cg = geo.ConjugateGradient().with_tolerance(1e-8).with_max_iterations(50000)
+    mixed = geo.ConjugateGradient().with_tolerance(1e-8).with_max_iterations(50000).with_precision("mixed")
+    op = geo.ElasticityOperator(mesh, dm, geo.IsotropicElasticity(1e11, 0.25), None, ctx)
+    u0 = np.zeros(3 * N)
+    out = {}
+    for name, fn in (("csr_fp64", lambda be: be.step(mesh, dm, mat, f_ext, csr_cg)),
+                     ("operator_mixed", lambda be: be.step_operator(op, mesh, f_ext, mixed))):
+        be = geo.BackwardEuler.new(3 * N, dt)
+        fn(be)  # warm
+        be.reset()
+        t0 = time.perf_counter()
+        u, ts = fn(be)
+        t1 = time.perf_counter()
+        geo.update_stresses_maxwell(mesh, dm, mat, u0, u, dt, ctx)
+        t2 = time.perf_counter()
+        out[name] = {"step_s": t1 - t0, "stress_update_s": t2 - t1, "iterations": ts.iterations}
+        out[name + "_u"] = u
+    out["step_speedup"] = out["csr_fp64"]["step_s"] / out["operator_mixed"]["step_s"]
+    ua, ub = out.pop("csr_fp64_u"), out.pop("operator_mixed_u")
+    out["solution_rel_l2"] = float(np.linalg.norm(ua - ub) / np.linalg.norm(ua))
+    out["config"] = "48x48x24 hexes (331,776 elements, 1,383,123 DOFs), one step, host-timed"
+    return out
 
 
 # --------------------------------------------------------------------------- reference arm

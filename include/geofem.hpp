@@ -187,6 +187,27 @@ struct IsotropicElasticity {
     static IsotropicElasticity new_(double E, double nu) { return {E, nu}; }
 };
 
+// mechanics/constitutive.rs:286-395
+struct MaxwellViscoelasticity {
+    double youngs_modulus;
+    double poisson_ratio;
+    double viscosity;
+    static MaxwellViscoelasticity new_(double E, double nu, double mu) {
+        if (!(E > 0) || !(nu > -1.0 && nu < 0.5) || !(mu > 0))
+            throw Error(GEO_ERR_INVALID_ARG, "invalid Maxwell material parameters");
+        return {E, nu, mu};
+    }
+    double shear_modulus() const { return youngs_modulus / (2.0 * (1.0 + poisson_ratio)); }
+    double relaxation_time() const { return viscosity / shear_modulus(); }
+};
+
+// mesh/state.rs:12-75: Voigt stress [xx yy zz xy yz zx] per element
+using Voigt = std::array<double, 6>;
+struct StressHistory {
+    std::vector<Voigt> stress;
+    explicit StressHistory(size_t n_elements = 0) : stress(n_elements, Voigt{0, 0, 0, 0, 0, 0}) {}
+};
+
 // ---------------------------------------------------------------- CSR
 class CsMat {
 public:
@@ -327,6 +348,26 @@ struct Assembler {
                                                     mat.poisson_ratio, &k));
         return CsMat(k, &ctx);
     }
+    // the history force of assemble_maxwell_viscoelastic_parallel (assembly.rs:959-1020)
+    static std::vector<double> maxwell_history_force(const Mesh& mesh, const StressHistory& sh,
+                                                     Context& ctx = Context::default_context()) {
+        size_check(sh.stress.size(), mesh.num_elements(), "stress history");
+        std::vector<double> f(3 * mesh.num_nodes());
+        ctx.check(geo_maxwell_history_force(ctx.get(), mesh.handle(ctx), sh.stress[0].data(), f.data()));
+        return f;
+    }
+    // assembly.rs:959-1020: (elastic K, f_history)
+    static std::pair<CsMat, std::vector<double>> assemble_maxwell_viscoelastic_parallel(
+        const Mesh& mesh, const DofManager& dofs, const MaxwellViscoelasticity& m, double dt, const StressHistory& sh,
+        Context& ctx = Context::default_context()) {
+        size_check(sh.stress.size(), mesh.num_elements(), "stress history");
+        geo_csr* k = nullptr;
+        std::vector<double> f(dofs.total_dofs());
+        ctx.check(geo_assemble_maxwell_viscoelastic(ctx.get(), mesh.handle(ctx), dofs.handle(ctx), m.youngs_modulus,
+                                                    m.poisson_ratio, m.viscosity, dt, sh.stress[0].data(), &k,
+                                                    f.data()));
+        return {CsMat(k, &ctx), std::move(f)};
+    }
     // assembly.rs:906-937
     static std::vector<double> assemble_gravity_load(const Mesh& mesh, const DofManager& dofs, double density,
                                                      const std::array<double, 3>& gravity,
@@ -347,6 +388,17 @@ private:
         if (got != want) throw Error(GEO_ERR_INVALID_ARG, std::string(what) + " has the wrong length");
     }
 };
+
+// mechanics/stress_update.rs:39-143: stresses after the step u_n -> u_next
+inline std::vector<Voigt> update_stresses_maxwell(const Mesh& mesh, const MaxwellViscoelasticity& m,
+                                                  const std::vector<double>& u_n, const std::vector<double>& u_next,
+                                                  double dt, const StressHistory& sh,
+                                                  Context& ctx = Context::default_context()) {
+    std::vector<Voigt> out(mesh.num_elements());
+    ctx.check(geo_update_stresses_maxwell(ctx.get(), mesh.handle(ctx), m.youngs_modulus, m.poisson_ratio, m.viscosity,
+                                          u_n.data(), u_next.data(), dt, sh.stress[0].data(), out[0].data()));
+    return out;
+}
 
 // ---------------------------------------------------------------- solver
 struct SolverStats {

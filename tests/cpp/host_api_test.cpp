@@ -118,6 +118,41 @@ void flux_profile() {
                " top faces)");
 }
 
+// maxwell_stress_relaxation.rs: held uniaxial stress, deviatoric part decays by 1/(1 + dt/tau) per step
+void maxwell_relaxation() {
+    const double E = 100e9, nu = 0.25, eps0 = 1e-3;
+    const MaxwellViscoelasticity m = MaxwellViscoelasticity::new_(E, nu, 1e19);
+    const double dt = 0.5 * m.relaxation_time();
+    Mesh mesh = ImprovedMeshGenerator::generate_cube(2, 2, 2, 1.0, 1.0, 1.0);
+    DofManager dofs(mesh.num_nodes(), 3);
+    for (size_t i = 0; i < mesh.num_nodes(); ++i) {
+        const double x = mesh.nodes[i][0], y = mesh.nodes[i][1], z = mesh.nodes[i][2];
+        const double dmin = std::fmin(std::fmin(std::fmin(x, 1 - x), std::fmin(y, 1 - y)), std::fmin(z, 1 - z));
+        if (dmin < 1e-6) {
+            dofs.set_dirichlet(dofs.global_dof(i, 0), -nu * eps0 * x);
+            dofs.set_dirichlet(dofs.global_dof(i, 1), -nu * eps0 * y);
+            dofs.set_dirichlet(dofs.global_dof(i, 2), eps0 * z);
+        }
+    }
+    StressHistory sh(mesh.num_elements());
+    const ConjugateGradient cg = ConjugateGradient().with_max_iterations(5000).with_tolerance(1e-12);
+    auto sys = Assembler::assemble_maxwell_viscoelastic_parallel(mesh, dofs, m, 1e-20, sh);
+    auto kb = Assembler::apply_dirichlet_bcs(sys.first, std::vector<double>(dofs.total_dofs(), 0.0), dofs);
+    std::vector<double> u = cg.solve(kb.first, kb.second).first;
+    sh.stress = update_stresses_maxwell(mesh, m, std::vector<double>(u.size(), 0.0), u, 1e-20, sh);
+    double worst = 0;
+    for (int k = 1; k <= 3; ++k) {
+        auto step = Assembler::assemble_maxwell_viscoelastic_parallel(mesh, dofs, m, dt, sh);
+        auto sb = Assembler::apply_dirichlet_bcs(step.first, step.second, dofs);
+        std::vector<double> un = cg.solve(sb.first, sb.second).first;
+        sh.stress = update_stresses_maxwell(mesh, m, u, un, dt, sh);
+        u = un;
+        const double p = E * eps0 / 3, expect = p + 2 * p * std::pow(1.0 + dt / m.relaxation_time(), -k);
+        for (const Voigt& s : sh.stress) worst = std::fmax(worst, std::fabs(s[2] - expect) / expect);
+    }
+    expect(worst < 1e-6, "Maxwell stress relaxation (3 backward-Euler steps): max rel error " + sci(worst));
+}
+
 void small_cg() {
     CsMat A = CsMat::from_arrays(2, 2, {0, 2, 4}, {0, 1, 0, 1}, {2.0, 1.0, 1.0, 2.0});
     auto s = ConjugateGradient().solve(A, {3.0, 3.0});
@@ -259,6 +294,7 @@ int main() {
         thermal_profile();
         patch_test();
         flux_profile();
+        maxwell_relaxation();
         errors();
         adjoint_fd();
     } catch (const Error& e) {
