@@ -267,6 +267,7 @@ def run_ours(args, ws, rank, local, pg):
         extras["elasticity_48x48x24"] = elasticity_config(ctx)
         extras["neumann_128"] = neumann_timing(ctx, mesh)
         extras["maxwell_step_48x48x24"] = maxwell_step(ctx)
+        extras["meshgen_128"] = meshgen_timing(ctx, n)
 
     # dominant kernel: the FP32 patch kernel in PCG mode, timed launch by launch with
     # CUDA events on the context stream right after the timed region
@@ -507,6 +508,35 @@ def neumann_timing(ctx, mesh):
     t2 = time.perf_counter()
     return {"faces": int(faces.shape[0]), "find_boundary_faces_s": t1 - t0, "apply_neumann_s": t2 - t1,
             "total_flux": float(f.sum()), "expected_total_flux": 0.05 * LX * LY}
+
+
+def meshgen_timing(ctx, n):
+    """ImprovedMeshGenerator::generate_cube at n^3 hexes: the host generator plus the
+    upload into a device mesh, against geo_mesh_generate_cube building the device
+    mesh in place (device time includes its allocations). The device mesh is copied
+    out once and compared with the host arrays bit for bit."""
+    import geo_simulator_b200 as geo
+    t0 = time.perf_counter()
+    hm = geo.ImprovedMeshGenerator.generate_cube(n, n, n, LX, LY, LZ)
+    t1 = time.perf_counter()
+    hm.handle(ctx)
+    t2 = time.perf_counter()
+    geo.ImprovedMeshGenerator.generate_cube_device(n, n, n, LX, LY, LZ, ctx)  # warm-up
+    reps = 3
+    t3 = time.perf_counter()
+    for _ in range(reps):
+        dm = geo.ImprovedMeshGenerator.generate_cube_device(n, n, n, LX, LY, LZ, ctx)
+        del dm
+    t4 = time.perf_counter()
+    dev_s, dm = _device_timed(ctx, lambda: geo.ImprovedMeshGenerator.generate_cube_device(n, n, n, LX, LY, LZ, ctx))
+    same = bool(np.array_equal(dm.elements, hm.elements)
+                and np.array_equal(dm.nodes.view(np.uint64), hm.nodes.view(np.uint64)))
+    out_bytes = 24 * dm.num_nodes() + 40 * dm.num_elements()
+    return {"nodes": dm.num_nodes(), "elements": dm.num_elements(),
+            "host_generate_s": t1 - t0, "host_upload_s": t2 - t1,
+            "device_generate_wall_s": (t4 - t3) / reps, "device_generate_events_s": dev_s,
+            "speedup_vs_host_generate_and_upload": (t2 - t0) / ((t4 - t3) / reps),
+            "device_mesh_bytes": out_bytes, "bit_exact_vs_host": same}
 
 
 def maxwell_step(ctx):

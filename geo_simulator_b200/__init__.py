@@ -9,7 +9,7 @@ of ``include/geo_fem.h`` (``libgeofem.so``).
 from .fem import (  # noqa: F401
     Assembler, BodyForce, BoundaryConditions, BoundaryFace, ConjugateGradient, Context, CsrMatrix, DofManager,
     ElasticityElement, ElasticityOperator, ElementMatrix, GeoError, ImprovedMeshGenerator, IsotropicElasticity,
-    MaxwellViscoelasticity, Mesh, NeumannBC, SolverStats, StressHistory, Tet10Face, ThermalOperator, BackwardEuler,
+    MaxwellViscoelasticity, Mesh, DeviceMesh, NeumannBC, SolverStats, StressHistory, Tet10Face, ThermalOperator, BackwardEuler,
     TimeStepStats, update_stresses_maxwell,
 )
 

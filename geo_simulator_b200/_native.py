@@ -70,6 +70,9 @@ _SIGS = {
     "geo_generate_cube": [_I64, _I64, _I64, _D, _D, _D, _DP, _DP],
     "geo_mesh_create": [_P, _I64, _DP, _I64, _DP, _PP],
     "geo_mesh_destroy": [_P],
+    "geo_mesh_generate_cube": [_P, _I64, _I64, _I64, _D, _D, _D, _PP],
+    "geo_mesh_size": [_P, C.POINTER(_I64), C.POINTER(_I64)],
+    "geo_mesh_download": [_P, _DP, _DP],
     "geo_dofs_create": [_P, _I64, _I32, _DP, _DP, _PP],
     "geo_dofs_num_dirichlet": [_P, C.POINTER(_I64)],
     "geo_dofs_destroy": [_P],

@@ -154,6 +154,67 @@ class ImprovedMeshGenerator:
         m.nodes, m.elements, m._handles, m.stress_history = xyz, conn, {}, None
         return m
 
+    @staticmethod
+    def generate_cube_device(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float, ctx=None) -> "DeviceMesh":
+        """``generate_cube`` run on the GPU: the mesh is built in device memory
+        (same numbering, coordinates and connectivity, bit for bit) and the host
+        arrays are only downloaded when ``nodes`` / ``elements`` are read."""
+        ctx = _ctx(ctx)
+        h = C.c_void_p()
+        ctx.check(N.lib().geo_mesh_generate_cube(ctx.h, nx, ny, nz, float(lx), float(ly), float(lz), C.byref(h)))
+        return DeviceMesh(ctx, h)
+
+
+class DeviceMesh(Mesh):
+    """A Mesh whose primary copy lives on the device (``geo_mesh``); ``nodes`` and
+    ``elements`` are the reference's host arrays, copied out on first access."""
+
+    def __init__(self, ctx, h):
+        n_nodes, n_elem = C.c_int64(), C.c_int64()
+        ctx.check(N.lib().geo_mesh_size(h, C.byref(n_nodes), C.byref(n_elem)))
+        self._n_nodes, self._n_elem = int(n_nodes.value), int(n_elem.value)
+        self._handles = {id(ctx): (ctx, h)}
+        self._ctx = ctx
+        self._nodes = self._elements = None
+        self.stress_history = None
+
+    def num_nodes(self) -> int:
+        return self._n_nodes
+
+    def num_elements(self) -> int:
+        return self._n_elem
+
+    def _download(self, nodes: bool):
+        h = self._handles[id(self._ctx)][1]
+        if nodes:
+            xyz = np.empty((self._n_nodes, 3), np.float64)
+            self._ctx.check(N.lib().geo_mesh_download(h, _ptr(xyz), None))
+            self._nodes = xyz
+        else:
+            conn = np.empty((self._n_elem, 10), np.int32)
+            self._ctx.check(N.lib().geo_mesh_download(h, None, _ptr(conn)))
+            self._elements = conn
+
+    @property
+    def nodes(self):
+        if self._nodes is None:
+            self._download(True)
+        return self._nodes
+
+    @nodes.setter
+    def nodes(self, value):
+        self._nodes = value
+
+    @property
+    def elements(self):
+        if self._elements is None:
+            self._download(False)
+        return self._elements
+
+    @elements.setter
+    def elements(self, value):
+        self._elements = value
+
 
 # --------------------------------------------------------------------------- DOFs
 class DofManager:

@@ -2,6 +2,7 @@
 
     python -m geo_simulator_b200.kernel_timing [--size 96] [--iterations 20]
         [--precision mixed|fp64] [--physics thermal|elasticity]
+    python -m geo_simulator_b200.kernel_timing --meshgen --size 128
 
 Builds the n^3-hex ImprovedMeshGenerator cube (1000 x 1000 x 600, ln k_e ~
 N(ln 3, 0.5^2) from seed 1001, T = 1280 at z = 0 and 0 at z = 600, Q = 1e-6;
@@ -11,6 +12,10 @@ geo_op_time_pcg_kernels (every launch does full work) and prints one JSON line
 with the patch-kernel and node-update times and their algorithmic bytes. Used
 for kernel profiles: its only launches of the PCG-mode patch kernel are the
 timed ones.
+
+With --meshgen it instead builds the same cube once on the device
+(geo_mesh_generate_cube: one launch each of k_cube_vertices, k_cube_midpoints
+and k_cube_conn) and prints its sizes and the mesh's algorithmic bytes.
 """
 from __future__ import annotations
 
@@ -34,6 +39,14 @@ def update_bytes(N, s, dpn=1):
     """Algorithmic bytes of one node-update launch: p, q, x, r, D^-1 read, x and r
     written, Dirichlet bitmask."""
     return N * dpn * 7 * s + N * dpn / 8
+
+
+def meshgen_bytes(n_nodes, n_elem, n_vertices):
+    """Algorithmic bytes of geo_mesh_generate_cube: coordinates (3 doubles per node)
+    and connectivity (10 int32 per element) written once, and the int32 edge-table
+    entry of every midpoint written once and read back once (the 6 reads per
+    element hit L2)."""
+    return 24 * n_nodes + 40 * n_elem + 8 * (n_nodes - n_vertices)
 
 
 def build(size, physics):
@@ -73,8 +86,17 @@ def main():
     ap.add_argument("--iterations", type=int, default=20)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--physics", default="thermal", choices=["thermal", "elasticity"])
+    ap.add_argument("--meshgen", action="store_true")
     args = ap.parse_args()
     from geo_simulator_b200 import _native as N
+    if args.meshgen:
+        import geo_simulator_b200 as geo
+        n = args.size
+        dm = geo.ImprovedMeshGenerator.generate_cube_device(n, n, n, LX, LY, LZ)
+        nv = (n + 1) ** 3
+        print(json.dumps({"size": n, "nodes": dm.num_nodes(), "elements": dm.num_elements(),
+                          "bytes": meshgen_bytes(dm.num_nodes(), dm.num_elements(), nv)}))
+        return
     mesh, op, fb = build(args.size, args.physics)
     prec = N.PRECISION_MIXED if args.precision == "mixed" else N.PRECISION_FP64
     pms, ums = C.c_double(), C.c_double()

@@ -111,6 +111,19 @@ int geo_mesh_create(geo_ctx* ctx, int64_t n_nodes, const double* xyz, int64_t n_
                     const int32_t* conn, geo_mesh** out);
 int geo_mesh_destroy(geo_mesh* mesh);
 
+/* ImprovedMeshGenerator::generate_cube, mesh_generator_improved.rs:19-169, run
+ * on the device: builds the device mesh directly (no host arrays, no upload)
+ * with the node numbering, coordinates and connectivity of geo_generate_cube,
+ * bit for bit. The reference returns a host Mesh; geo_mesh_download gives that. */
+int geo_mesh_generate_cube(geo_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, double lx, double ly, double lz,
+                           geo_mesh** out);
+/* Node and element counts of a device mesh (Mesh::num_nodes / num_elements,
+ * mesh/geometry.rs). Either pointer may be NULL.                               */
+int geo_mesh_size(const geo_mesh* mesh, int64_t* n_nodes, int64_t* n_elem);
+/* Copies a device mesh out in the layout of geo_generate_cube: xyz[n_nodes][3]
+ * and conn[n_elem][10], host or device memory; either may be NULL.             */
+int geo_mesh_download(const geo_mesh* mesh, double* xyz, int32_t* conn);
+
 /* DofManager::new + set_dirichlet, dof.rs:37-50, :113-130. dirichlet_mask[n_dofs]
  * (nonzero = constrained) and dirichlet_values[n_dofs]; either may be NULL.     */
 int geo_dofs_create(geo_ctx* ctx, int64_t n_nodes, int32_t dofs_per_node,

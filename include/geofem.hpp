@@ -4,7 +4,7 @@
 //
 //   reference (Rust)                                   here (C++)
 //   ImprovedMeshGenerator::generate_cube(..)           geofem::ImprovedMeshGenerator::generate_cube(..)
-//     (src/mesh/mesh_generator_improved.rs:19-169)
+//     (src/mesh/mesh_generator_improved.rs:19-169)        and generate_cube_device(ctx, ..) (on the GPU)
 //   DofManager::new(n, dpn), set_dirichlet(_node)      geofem::DofManager(n, dpn), set_dirichlet(_node)
 //     (src/fem/dof.rs:37-140)
 //   Assembler::assemble_thermal_stiffness_parallel     geofem::Assembler::assemble_thermal_stiffness_parallel
@@ -95,11 +95,35 @@ public:
 
     Mesh() = default;
     Mesh(std::vector<Point3> n, std::vector<Tet10> e) : nodes(std::move(n)), elements(std::move(e)) {}
-    size_t num_nodes() const { return nodes.size(); }
-    size_t num_elements() const { return elements.size(); }
-    void invalidate() { dev_.reset(); }
+    // A mesh that exists only on the device (ImprovedMeshGenerator::generate_cube_device):
+    // nodes/elements stay empty until download() copies them out.
+    static Mesh from_device(Context& ctx, geo_mesh* m) {
+        Mesh out;
+        out.dev_.reset(m, [](geo_mesh* p) { geo_mesh_destroy(p); });
+        out.dev_ctx_ = ctx.get();
+        int64_t nn = 0, ne = 0;
+        ctx.check(geo_mesh_size(m, &nn, &ne));
+        out.dev_nodes_ = (size_t)nn;
+        out.dev_elems_ = (size_t)ne;
+        return out;
+    }
+    size_t num_nodes() const { return nodes.empty() && dev_ ? dev_nodes_ : nodes.size(); }
+    size_t num_elements() const { return elements.empty() && dev_ ? dev_elems_ : elements.size(); }
+    bool host_resident() const { return !nodes.empty() || !dev_; }
+    // Fills nodes/elements from the device copy (no-op for a host mesh).
+    void download(Context& ctx) {
+        if (host_resident()) return;
+        nodes.resize(dev_nodes_);
+        elements.resize(dev_elems_);
+        ctx.check(geo_mesh_download(dev_.get(), nodes[0].data(), elements[0].data()));
+    }
+    void invalidate() {
+        if (host_resident()) dev_.reset();
+    }
 
     const geo_mesh* handle(Context& ctx) const {
+        if (dev_ && !host_resident() && dev_ctx_ != ctx.get())
+            throw Error(GEO_ERR_INVALID_ARG, "device-only mesh used with another context: download() it first");
         if (!dev_ || dev_ctx_ != ctx.get()) {
             geo_mesh* m = nullptr;
             ctx.check(geo_mesh_create(ctx.get(), (int64_t)nodes.size(), nodes.empty() ? nullptr : nodes[0].data(),
@@ -114,6 +138,7 @@ public:
 private:
     mutable std::shared_ptr<geo_mesh> dev_;
     mutable const geo_ctx* dev_ctx_ = nullptr;
+    size_t dev_nodes_ = 0, dev_elems_ = 0;
 };
 
 struct ImprovedMeshGenerator {
@@ -128,6 +153,13 @@ struct ImprovedMeshGenerator {
         rc = geo_generate_cube(nx, ny, nz, lx, ly, lz, m.nodes[0].data(), m.elements[0].data());
         if (rc != GEO_OK) throw Error(rc, "generate_cube failed");
         return m;
+    }
+    // The same mesh built in device memory (geo_mesh_generate_cube); see Mesh::from_device.
+    static Mesh generate_cube_device(Context& ctx, int64_t nx, int64_t ny, int64_t nz, double lx, double ly,
+                                     double lz) {
+        geo_mesh* m = nullptr;
+        ctx.check(geo_mesh_generate_cube(ctx.get(), nx, ny, nz, lx, ly, lz, &m));
+        return Mesh::from_device(ctx, m);
     }
 };
 
@@ -290,6 +322,8 @@ struct Assembler {
     static std::vector<BoundaryFace> find_boundary_faces(const Mesh& mesh,
                                                          const std::function<bool(const Point3&)>& condition,
                                                          Context& ctx = Context::default_context()) {
+        if (!mesh.host_resident())
+            throw Error(GEO_ERR_INVALID_ARG, "find_boundary_faces needs node coordinates: download() the mesh first");
         std::vector<uint8_t> mask(mesh.num_nodes());
         for (size_t i = 0; i < mask.size(); ++i) mask[i] = condition(mesh.nodes[i]) ? 1 : 0;
         int64_t n = 0;

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -281,6 +282,28 @@ void adjoint_fd() {
     expect(ok, "adjoint dJ/d(ln k_e) agrees with central finite differences to 1e-5");
 }
 
+void device_mesh() {
+    Context& ctx = Context::default_context();
+    const Mesh hm = ImprovedMeshGenerator::generate_cube(5, 4, 3, 1000, 800, 600);
+    Mesh dm = ImprovedMeshGenerator::generate_cube_device(ctx, 5, 4, 3, 1000, 800, 600);
+    expect(!dm.host_resident() && dm.num_nodes() == hm.num_nodes() && dm.num_elements() == hm.num_elements(),
+           "device mesh: sizes without a host copy");
+    DofManager dofs(hm.num_nodes(), 1);
+    const CsMat Kh = Assembler::assemble_thermal_stiffness_parallel(hm, dofs, 2.0);
+    const CsMat Kd = Assembler::assemble_thermal_stiffness_parallel(dm, dofs, 2.0);
+    std::vector<int64_t> ph, pd;
+    std::vector<int32_t> ih, id;
+    std::vector<double> vh, vd;
+    Kh.to_host(ph, ih, vh);
+    Kd.to_host(pd, id, vd);
+    expect(ph == pd && ih == id && vh == vd, "device mesh assembles the same CSR as the host mesh");
+    dm.download(ctx);
+    bool same = dm.elements == hm.elements && dm.nodes.size() == hm.nodes.size();
+    for (size_t i = 0; same && i < hm.nodes.size(); ++i)
+        same = std::memcmp(dm.nodes[i].data(), hm.nodes[i].data(), sizeof(Point3)) == 0;
+    expect(same, "device mesh downloads bit-identical to the host generator");
+}
+
 }  // namespace
 
 int main() {
@@ -297,6 +320,7 @@ int main() {
         maxwell_relaxation();
         errors();
         adjoint_fd();
+        device_mesh();
     } catch (const Error& e) {
         std::printf("FAIL unexpected geofem::Error %d: %s\n", e.code(), e.what());
         return 1;
