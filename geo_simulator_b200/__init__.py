@@ -10,7 +10,7 @@ from .fem import (  # noqa: F401
     Assembler, BodyForce, BoundaryConditions, BoundaryFace, ConjugateGradient, Context, CsrMatrix, DofManager,
     ElasticityElement, ElasticityOperator, ElementMatrix, GeoError, ImprovedMeshGenerator, IsotropicElasticity,
     MaxwellViscoelasticity, Mesh, DeviceMesh, NeumannBC, SolverStats, StressHistory, Tet10Face, ThermalOperator, BackwardEuler,
-    TimeStepStats, update_stresses_maxwell,
+    TimeStepStats, update_stresses_maxwell, FieldData, ScalarField, VectorField, VtkWriter,
 )
 
 __version__ = "0.1.0"

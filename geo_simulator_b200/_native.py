@@ -73,6 +73,8 @@ _SIGS = {
     "geo_mesh_generate_cube": [_P, _I64, _I64, _I64, _D, _D, _D, _PP],
     "geo_mesh_size": [_P, C.POINTER(_I64), C.POINTER(_I64)],
     "geo_mesh_download": [_P, _DP, _DP],
+    "geo_vtu_render": [_P, _P, _P, _I32, _P, _I32, _DP, _I64, C.POINTER(_I64)],
+    "geo_write_vtu": [_P, _P, _P, _I32, _P, _I32, C.c_char_p, C.POINTER(_I64)],
     "geo_dofs_create": [_P, _I64, _I32, _DP, _DP, _PP],
     "geo_dofs_num_dirichlet": [_P, C.POINTER(_I64)],
     "geo_dofs_destroy": [_P],

@@ -114,6 +114,7 @@ class Mesh:
         self.elements = np.ascontiguousarray(el, dtype=np.int32).reshape(-1, 10)
         self._handles = {}
         self.stress_history = None  # StressHistory for viscoelasticity (mesh/geometry.rs)
+        self.field_data, self.cell_data = FieldData(), FieldData()  # mesh/geometry.rs:44-45
 
     def num_nodes(self) -> int:
         return int(self.nodes.shape[0])
@@ -152,6 +153,7 @@ class ImprovedMeshGenerator:
         N.check(L.geo_generate_cube(nx, ny, nz, float(lx), float(ly), float(lz), _ptr(xyz), _ptr(conn)))
         m = Mesh.__new__(Mesh)
         m.nodes, m.elements, m._handles, m.stress_history = xyz, conn, {}, None
+        m.field_data, m.cell_data = FieldData(), FieldData()
         return m
 
     @staticmethod
@@ -177,6 +179,7 @@ class DeviceMesh(Mesh):
         self._ctx = ctx
         self._nodes = self._elements = None
         self.stress_history = None
+        self.field_data, self.cell_data = FieldData(), FieldData()
 
     def num_nodes(self) -> int:
         return self._n_nodes
@@ -214,6 +217,132 @@ class DeviceMesh(Mesh):
     @elements.setter
     def elements(self, value):
         self._elements = value
+
+
+# --------------------------------------------------------------------------- fields and VTU output
+class ScalarField:
+    """mesh/fields.rs:4-26: a named value per node (or per cell)."""
+
+    def __init__(self, name: str, data):
+        self.name, self.data = str(name), data
+
+    new = classmethod(lambda cls, name, data: cls(name, data))
+
+    def len(self) -> int:
+        return int(np.asarray(self.data).size) if not hasattr(self.data, "numel") else int(self.data.numel())
+
+
+class VectorField:
+    """mesh/fields.rs:28-76: a named 3-vector per node (or per cell), stored [n][3]."""
+
+    def __init__(self, name: str, data):
+        self.name, self.data = str(name), data
+
+    new = classmethod(lambda cls, name, data: cls(name, data))
+
+    @classmethod
+    def from_dof_vector(cls, name: str, dof_vector):
+        """fields.rs:54-66: interleaved [x0 y0 z0 x1 ...]; panics unless 3 | len."""
+        n = dof_vector.numel() if hasattr(dof_vector, "numel") else np.asarray(dof_vector).size
+        if n % 3:
+            raise GeoError(N.GEO_ERR_INVALID_ARG, "DOF vector must have 3*n entries for vector field")
+        return cls(name, dof_vector)
+
+    def len(self) -> int:
+        n = self.data.numel() if hasattr(self.data, "numel") else np.asarray(self.data).size
+        return int(n) // 3
+
+
+class FieldData:
+    """mesh/fields.rs:78-137. The reference keys HashMaps (unspecified order);
+    these dicts keep insertion order, which VtkWriter writes."""
+
+    def __init__(self):
+        self.scalar_fields: dict[str, ScalarField] = {}
+        self.vector_fields: dict[str, VectorField] = {}
+
+    new = classmethod(lambda cls: cls())
+
+    def add_field(self, field: ScalarField):
+        self.scalar_fields[field.name] = field
+
+    def add_vector_field(self, field: VectorField):
+        self.vector_fields[field.name] = field
+
+    def get_field(self, name):
+        return self.scalar_fields.get(name)
+
+    def get_vector_field(self, name):
+        return self.vector_fields.get(name)
+
+    def field_names(self):
+        return list(self.scalar_fields)
+
+    def vector_field_names(self):
+        return list(self.vector_fields)
+
+    def num_fields(self) -> int:
+        return len(self.scalar_fields)
+
+    def num_vector_fields(self) -> int:
+        return len(self.vector_fields)
+
+    def is_empty(self) -> bool:
+        return not self.scalar_fields and not self.vector_fields
+
+
+class _VtuField(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("data", C.c_void_p), ("count", C.c_int64), ("components", C.c_int32)]
+
+
+def _vtu_fields(fd: FieldData):
+    keep, out = [], []
+    for f, comps in [(f, 1) for f in fd.scalar_fields.values()] + [(f, 3) for f in fd.vector_fields.values()]:
+        d = f.data
+        if hasattr(d, "is_cuda"):
+            d = d.detach().to(dtype=__import__("torch").float64).contiguous()
+            n = d.numel()
+        else:
+            d = np.ascontiguousarray(d, dtype=np.float64).reshape(-1)
+            n = d.size
+        keep.append(d)
+        out.append(_VtuField(f.name.encode(), _ptr(d), n // comps, comps))
+    arr = (_VtuField * max(1, len(out)))(*out)
+    return arr, len(out), keep
+
+
+class VtkWriter:
+    """mesh/vtk_writer.rs:7-265: ``write_vtu`` renders the text on the GPU, byte for
+    byte as the reference (Rust ``{}`` for every number)."""
+
+    @staticmethod
+    def write_vtu(mesh: Mesh, filename: str, ctx=None) -> int:
+        """VtkWriter::write_vtu (vtk_writer.rs:104-265); returns the bytes written."""
+        ctx = _ctx(ctx)
+        pf, npf, k1 = _vtu_fields(mesh.field_data)
+        cf, ncf, k2 = _vtu_fields(mesh.cell_data)
+        size = C.c_int64()
+        ctx.check(N.lib().geo_write_vtu(ctx.h, mesh.handle(ctx), pf, npf, cf, ncf, str(filename).encode(),
+                                        C.byref(size)))
+        return int(size.value)
+
+    @staticmethod
+    def render_vtu(mesh: Mesh, out=None, ctx=None):
+        """The same text as bytes (out None), or into ``out`` (a uint8 numpy array or
+        CUDA tensor large enough); returns the bytes or the size."""
+        ctx = _ctx(ctx)
+        pf, npf, k1 = _vtu_fields(mesh.field_data)
+        cf, ncf, k2 = _vtu_fields(mesh.cell_data)
+        L = N.lib()
+        size = C.c_int64()
+        if out is not None:
+            cap = out.numel() if hasattr(out, "numel") else out.size
+            ctx.check(L.geo_vtu_render(ctx.h, mesh.handle(ctx), pf, npf, cf, ncf, _ptr(out), cap, C.byref(size)))
+            return int(size.value)
+        ctx.check(L.geo_vtu_render(ctx.h, mesh.handle(ctx), pf, npf, cf, ncf, None, 0, C.byref(size)))
+        buf = np.empty(int(size.value), np.uint8)
+        ctx.check(L.geo_vtu_render(ctx.h, mesh.handle(ctx), pf, npf, cf, ncf, _ptr(buf), buf.size, C.byref(size)))
+        return buf.tobytes()
 
 
 # --------------------------------------------------------------------------- DOFs

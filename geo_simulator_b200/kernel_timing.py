@@ -3,6 +3,7 @@
     python -m geo_simulator_b200.kernel_timing [--size 96] [--iterations 20]
         [--precision mixed|fp64] [--physics thermal|elasticity]
     python -m geo_simulator_b200.kernel_timing --meshgen --size 128
+    python -m geo_simulator_b200.kernel_timing --vtu --size 128 [--vtu-file PATH]
 
 Builds the n^3-hex ImprovedMeshGenerator cube (1000 x 1000 x 600, ln k_e ~
 N(ln 3, 0.5^2) from seed 1001, T = 1280 at z = 0 and 0 at z = 600, Q = 1e-6;
@@ -16,6 +17,11 @@ timed ones.
 With --meshgen it instead builds the same cube once on the device
 (geo_mesh_generate_cube: one launch each of k_cube_vertices, k_cube_midpoints
 and k_cube_conn) and prints its sizes and the mesh's algorithmic bytes.
+
+With --vtu it builds that device mesh, attaches a seeded temperature field
+(N(600, 300^2) per node, seed 9) and renders the VTU text into a device buffer
+(geo_vtu_render: per section one k_item_lengths and one k_item_write launch),
+timed with CUDA events, then optionally streams the same text to a file.
 """
 from __future__ import annotations
 
@@ -47,6 +53,57 @@ def meshgen_bytes(n_nodes, n_elem, n_vertices):
     entry of every midpoint written once and read back once (the 6 reads per
     element hit L2)."""
     return 24 * n_nodes + 40 * n_elem + 8 * (n_nodes - n_vertices)
+
+
+def render_device(ctx, mesh, reps=3):
+    """geo_vtu_render of the mesh and its fields into a device buffer: (bytes, best
+    seconds of reps by CUDA events on the context stream)."""
+    import torch
+
+    from geo_simulator_b200 import _native as N
+    from geo_simulator_b200.fem import _vtu_fields
+    pf, npf, keep_p = _vtu_fields(mesh.field_data)
+    cf, ncf, keep_c = _vtu_fields(mesh.cell_data)
+    h = mesh.handle(ctx)
+    nbytes = C.c_int64()
+    ctx.check(N.lib().geo_vtu_render(ctx.h, h, pf, npf, cf, ncf, None, 0, C.byref(nbytes)))
+    size = int(nbytes.value)
+    buf = torch.empty(size, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    best = None
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.check(N.lib().geo_vtu_render(ctx.h, h, pf, npf, cf, ncf, buf.data_ptr(), size, C.byref(nbytes)))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        best = t if best is None else min(best, t)
+    return size, best
+
+
+def vtu_timing(n, path=None):
+    """The n^3 cube with a seeded temperature field: device render (render_device)
+    and, if path is given, the streamed write to that file (wall clock)."""
+    import time
+
+    import torch
+
+    import geo_simulator_b200 as geo
+    ctx = geo.Context.default()
+    dm = geo.ImprovedMeshGenerator.generate_cube_device(n, n, n, LX, LY, LZ, ctx)
+    T = np.random.default_rng(9).normal(600.0, 300.0, dm.num_nodes())
+    dm.field_data.add_field(geo.ScalarField("Temperature", torch.from_numpy(T).cuda()))
+    size, best = render_device(ctx, dm)
+    out = {"size": n, "nodes": dm.num_nodes(), "elements": dm.num_elements(), "bytes": size,
+           "render_device_s": best, "render_gbs": size / best / 1e9}
+    if path:
+        t0 = time.perf_counter()
+        geo.VtkWriter.write_vtu(dm, path, ctx)
+        out["write_file_s"] = time.perf_counter() - t0
+        out["write_file_gbs"] = size / out["write_file_s"] / 1e9
+    return out
 
 
 def build(size, physics):
@@ -87,8 +144,13 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--physics", default="thermal", choices=["thermal", "elasticity"])
     ap.add_argument("--meshgen", action="store_true")
+    ap.add_argument("--vtu", action="store_true")
+    ap.add_argument("--vtu-file", default=None)
     args = ap.parse_args()
     from geo_simulator_b200 import _native as N
+    if args.vtu:
+        print(json.dumps(vtu_timing(args.size, args.vtu_file)))
+        return
     if args.meshgen:
         import geo_simulator_b200 as geo
         n = args.size

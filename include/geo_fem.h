@@ -124,6 +124,31 @@ int geo_mesh_size(const geo_mesh* mesh, int64_t* n_nodes, int64_t* n_elem);
  * and conn[n_elem][10], host or device memory; either may be NULL.             */
 int geo_mesh_download(const geo_mesh* mesh, double* xyz, int32_t* conn);
 
+/* ------------------------------------------------------------------ VTU output */
+/* A point or cell field of VtkWriter::write_vtu (mesh/fields.rs ScalarField /
+ * VectorField). components 1: count values; components 3: count [x y z]
+ * triples (VectorField::from_dof_vector layout). data is host or device
+ * memory; name is written verbatim into Name="...".                            */
+typedef struct geo_vtu_field {
+    const char* name;
+    const double* data;
+    int64_t count;
+    int32_t components;
+} geo_vtu_field;
+
+/* VtkWriter::write_vtu, mesh/vtk_writer.rs:104-265, byte for byte: the ASCII
+ * VTU text of the mesh and its fields, formatted on the GPU (every f64 as Rust's
+ * `{}`: shortest round-trip digits, positional). Scalar fields are written
+ * before vector fields, each in the order given (the reference's two loops over
+ * its field maps). *size receives the byte count; with out == NULL nothing is
+ * written, otherwise out (host or device memory) must hold capacity >= *size
+ * bytes, else GEO_ERR_INVALID_ARG with *size still set.                       */
+int geo_vtu_render(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point_fields, int32_t n_point,
+                   const geo_vtu_field* cell_fields, int32_t n_cell, char* out, int64_t capacity, int64_t* size);
+/* The same text streamed to the file `path` (created or truncated); size may be NULL. */
+int geo_write_vtu(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point_fields, int32_t n_point,
+                  const geo_vtu_field* cell_fields, int32_t n_cell, const char* path, int64_t* size);
+
 /* DofManager::new + set_dirichlet, dof.rs:37-50, :113-130. dirichlet_mask[n_dofs]
  * (nonzero = constrained) and dirichlet_values[n_dofs]; either may be NULL.     */
 int geo_dofs_create(geo_ctx* ctx, int64_t n_nodes, int32_t dofs_per_node,

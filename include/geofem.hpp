@@ -16,6 +16,8 @@
 //     (src/linalg/iterative.rs:7-147)
 //   SolverStats (src/linalg/solver.rs:5-32)            geofem::SolverStats
 //   CsMat<f64> (sprs)                                  geofem::CsMat (device-resident CSR)
+//   FieldData / ScalarField / VectorField (mesh/fields.rs) geofem::FieldData / ScalarField / VectorField
+//   VtkWriter::write_vtu (mesh/vtk_writer.rs:104-265)  geofem::VtkWriter::write_vtu / render_vtu (GPU text)
 //
 // plus the matrix-free operators, the mixed-precision solve and the adjoint
 // (geofem::ThermalOperator / ElasticityOperator with forward and vjp), which
@@ -88,10 +90,48 @@ private:
 using Point3 = std::array<double, 3>;
 using Tet10 = std::array<int32_t, 10>;  // [v0 v1 v2 v3 e01 e12 e20 e03 e13 e23]
 
+// mesh/fields.rs:4-137. The reference keys HashMaps (iteration order unspecified);
+// these keep insertion order, which VtkWriter writes.
+struct ScalarField {
+    std::string name;
+    std::vector<double> data;
+};
+struct VectorField {
+    std::string name;
+    std::vector<Point3> data;
+    // fields.rs:54-66: interleaved [x0 y0 z0 x1 ...]
+    static VectorField from_dof_vector(const std::string& name, const std::vector<double>& dofs) {
+        if (dofs.size() % 3) throw std::invalid_argument("DOF vector must have 3*n entries for vector field");
+        VectorField f{name, std::vector<Point3>(dofs.size() / 3)};
+        for (size_t i = 0; i < f.data.size(); ++i) f.data[i] = {dofs[3 * i], dofs[3 * i + 1], dofs[3 * i + 2]};
+        return f;
+    }
+};
+struct FieldData {
+    std::vector<ScalarField> scalar_fields;
+    std::vector<VectorField> vector_fields;
+    void add_field(ScalarField f) { put(scalar_fields, std::move(f)); }
+    void add_vector_field(VectorField f) { put(vector_fields, std::move(f)); }
+    bool is_empty() const { return scalar_fields.empty() && vector_fields.empty(); }
+
+private:
+    template <class F>
+    static void put(std::vector<F>& v, F f) {  // HashMap::insert: a field of the same name is replaced
+        for (auto& g : v)
+            if (g.name == f.name) {
+                g = std::move(f);
+                return;
+            }
+        v.push_back(std::move(f));
+    }
+};
+
 class Mesh {
 public:
     std::vector<Point3> nodes;     // geometry.nodes
     std::vector<Tet10> elements;   // connectivity.tet10_elements
+    FieldData field_data;          // point data written by VtkWriter
+    FieldData cell_data;           // cell data written by VtkWriter
 
     Mesh() = default;
     Mesh(std::vector<Point3> n, std::vector<Tet10> e) : nodes(std::move(n)), elements(std::move(e)) {}
@@ -161,6 +201,42 @@ struct ImprovedMeshGenerator {
         ctx.check(geo_mesh_generate_cube(ctx.get(), nx, ny, nz, lx, ly, lz, &m));
         return Mesh::from_device(ctx, m);
     }
+};
+
+// mesh/vtk_writer.rs:104-265: the VTU text rendered on the GPU, byte for byte.
+struct VtkWriter {
+    static size_t write_vtu(const Mesh& mesh, const std::string& filename,
+                            Context& ctx = Context::default_context()) {
+        Fields f(mesh);
+        int64_t size = 0;
+        ctx.check(geo_write_vtu(ctx.get(), mesh.handle(ctx), f.point.data(), (int32_t)f.point.size(), f.cell.data(),
+                                (int32_t)f.cell.size(), filename.c_str(), &size));
+        return (size_t)size;
+    }
+    static std::string render_vtu(const Mesh& mesh, Context& ctx = Context::default_context()) {
+        Fields f(mesh);
+        int64_t size = 0;
+        ctx.check(geo_vtu_render(ctx.get(), mesh.handle(ctx), f.point.data(), (int32_t)f.point.size(), f.cell.data(),
+                                 (int32_t)f.cell.size(), nullptr, 0, &size));
+        std::string out((size_t)size, '\0');
+        ctx.check(geo_vtu_render(ctx.get(), mesh.handle(ctx), f.point.data(), (int32_t)f.point.size(), f.cell.data(),
+                                 (int32_t)f.cell.size(), &out[0], size, &size));
+        return out;
+    }
+
+private:
+    struct Fields {
+        std::vector<geo_vtu_field> point, cell;
+        explicit Fields(const Mesh& m) {
+            add(point, m.field_data);
+            add(cell, m.cell_data);
+        }
+        static void add(std::vector<geo_vtu_field>& v, const FieldData& fd) {
+            for (const auto& f : fd.scalar_fields) v.push_back({f.name.c_str(), f.data.data(), (int64_t)f.data.size(), 1});
+            for (const auto& f : fd.vector_fields)
+                v.push_back({f.name.c_str(), f.data.empty() ? nullptr : f.data[0].data(), (int64_t)f.data.size(), 3});
+        }
+    };
 };
 
 class DofManager {

@@ -125,6 +125,15 @@ int orc_update_stresses_maxwell(int64_t n_nodes, const double* xyz, int64_t n_el
                                 double nu, double mu, const double* u_n, const double* u_next, double dt,
                                 const double* stress_n, double* stress_next);
 
+/* ---- VTU output: mesh/vtk_writer.rs:104-265 with Rust's `{}` for f64 (oracle/vtu.cpp) ---- */
+/* Rust Display of one f64 into out (NUL-terminated); returns its length, -1 if cap is too small. */
+int orc_format_f64(double v, char* out, int cap);
+/* The whole file; returns its size and copies it to out when cap suffices. conn is [E][10]. */
+int64_t orc_write_vtu(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn, int n_point,
+                      const char* const* p_names, const double* const* p_data, const int64_t* p_counts,
+                      const int32_t* p_comps, int n_cell, const char* const* c_names, const double* const* c_data,
+                      const int64_t* c_counts, const int32_t* c_comps, char* out, int64_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,6 +103,10 @@ def _declare(L):
         "orc_maxwell_history_force": (C.c_int, [C.c_int64, _D, C.c_int64, _I64, _D, _D]),
         "orc_update_stresses_maxwell": (C.c_int, [C.c_int64, _D, C.c_int64, _I64, C.c_double, C.c_double,
                                                   C.c_double, _D, _D, C.c_double, _D, _D]),
+        "orc_format_f64": (C.c_int, [C.c_double, C.c_char_p, C.c_int]),
+        "orc_write_vtu": (C.c_int64, [C.c_int64, _D, C.c_int64, _I64, C.c_int, C.c_void_p, C.c_void_p, _I64,
+                                      C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _I64, C.c_void_p,
+                                      C.c_char_p, C.c_int64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -498,3 +502,38 @@ def thermal_bc(xyz, lz, t_bottom=1280.0, t_top=0.0):
     mask = (bottom | top).astype(np.uint8)
     vals = np.where(bottom, t_bottom, np.where(top, t_top, 0.0))
     return mask, vals
+
+
+# ------------------------------------------------------------------- VTU output
+def format_f64(v) -> str:
+    """Rust's `{}` for one f64 (core::fmt Display), see vtu.cpp."""
+    buf = C.create_string_buffer(400)
+    n = lib().orc_format_f64(float(v), buf, 400)
+    assert n >= 0
+    return buf.raw[:n].decode()
+
+
+def _field_arrays(fields):
+    n = len(fields)
+    names = (C.c_char_p * max(n, 1))(*[f[0].encode() for f in fields])
+    arrs = [_f64(np.asarray(f[1]).reshape(-1)) for f in fields]
+    ptrs = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in arrs])
+    comps = np.array([f[2] if len(f) > 2 else 1 for f in fields] or [1], np.int32)
+    counts = np.array([a.size // int(c) for a, c in zip(arrs, comps)] or [0], np.int64)
+    return n, names, ptrs, counts, comps, arrs
+
+
+def write_vtu(xyz, conn, point_fields=(), cell_fields=()) -> bytes:
+    """VtkWriter::write_vtu (mesh/vtk_writer.rs:104-265) as bytes. Fields are
+    (name, data, components) with components 1 (scalar) or 3 (vector, [n][3])."""
+    xyz = _f64(xyz)
+    conn = _i64(conn)
+    np_, pn, pp, pc, pk, keep_p = _field_arrays(list(point_fields))
+    nc, cn, cp, cc, ck, keep_c = _field_arrays(list(cell_fields))
+    L = lib()
+    args = (xyz.shape[0], _d(xyz), conn.shape[0], _i(conn), np_, pn, pp, _i(pc), pk.ctypes.data, nc, cn, cp,
+            _i(cc), ck.ctypes.data)
+    size = L.orc_write_vtu(*args, None, 0)
+    out = C.create_string_buffer(int(size))
+    L.orc_write_vtu(*args, out, size)
+    return out.raw[:size]

@@ -304,6 +304,34 @@ void device_mesh() {
     expect(same, "device mesh downloads bit-identical to the host generator");
 }
 
+void vtu_output() {
+    Mesh mesh = ImprovedMeshGenerator::generate_cube(2, 1, 1, 1000, 800, 600);
+    std::vector<double> t(mesh.num_nodes(), 1.0);
+    t[0] = 0.1 + 0.2;
+    t[1] = -0.0;
+    t[2] = 1e21;
+    mesh.field_data.add_field({"T", t});
+    mesh.cell_data.add_vector_field(VectorField::from_dof_vector("q", std::vector<double>(3 * mesh.num_elements(), 2.5e-7)));
+    const std::string text = VtkWriter::render_vtu(mesh);
+    expect(text.find("    <Piece NumberOfPoints=\"45\" NumberOfCells=\"12\">\n") != std::string::npos &&
+               text.find("          0 0 0\n          500 0 0\n          1000 0 0\n") != std::string::npos,
+           "VTU header and points as Rust prints them");
+    expect(text.find("          0.30000000000000004 -0 1000000000000000000000 1 ") != std::string::npos &&
+               text.find("0.00000025 0.00000025 0.00000025 ") != std::string::npos,
+           "VTU field values printed as Rust's Display");
+    const char* path = "host_api_test_out.vtu";
+    const size_t n = VtkWriter::write_vtu(mesh, path);
+    std::string back;
+    if (FILE* fp = std::fopen(path, "rb")) {
+        char buf[4096];
+        size_t k;
+        while ((k = std::fread(buf, 1, sizeof buf, fp)) > 0) back.append(buf, k);
+        std::fclose(fp);
+    }
+    std::remove(path);
+    expect(n == text.size() && back == text, "write_vtu streams the same bytes as render_vtu");
+}
+
 }  // namespace
 
 int main() {
@@ -321,6 +349,7 @@ int main() {
         errors();
         adjoint_fd();
         device_mesh();
+        vtu_output();
     } catch (const Error& e) {
         std::printf("FAIL unexpected geofem::Error %d: %s\n", e.code(), e.what());
         return 1;

@@ -18,9 +18,9 @@ def test_host_api_builds_and_links():
 
 
 @pytest.mark.gpu
-def test_host_api_on_gpu():
+def test_host_api_on_gpu(tmp_path):
     subprocess.run(["make", "-s", "-C", CPP], check=True)
-    r = subprocess.run([BIN], capture_output=True, text=True, timeout=600)
+    r = subprocess.run([BIN], capture_output=True, text=True, timeout=600, cwd=str(tmp_path))
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "PASSED: 0 failure(s)" in r.stdout
