@@ -278,28 +278,30 @@ int geo_apply_neumann_bcs(geo_ctx* ctx, const geo_mesh* mesh, int64_t n_faces, c
     GEO_CHECK_ARG(6 * n_faces < INT32_MAX, "too many faces");
     cudaStream_t s = ctx->stream;
     const int64_t m = 6 * n_faces;
-    DevBuf<int32_t> tf, keys(m), keys2(m), idx(m), idx2(m);
-    DevBuf<double> tq, contrib(m), fd;
-    const int32_t* df = stage_faces(faces, n_faces, tf, s);
-    const double* dq = flux_f ? stage_in(flux_f, (size_t)n_faces, tq, s) : nullptr;
+    // per-call temporaries in the context scratch (this runs every step of a transient)
+    const int64_t m_al = (m + 63) & ~int64_t(63);
+    int32_t* keys = ctx_scratch<int32_t>(ctx, SCR_TMP0, (size_t)(4 * m_al));
+    int32_t *keys2 = keys + m_al, *idx = keys2 + m_al, *idx2 = idx + m_al;
+    double* contrib = ctx_scratch<double>(ctx, SCR_TMP1, (size_t)m);
+    const int32_t* df = stage_in(ctx, SCR_IN0, faces, (size_t)(2 * n_faces));
+    const double* dq = flux_f ? stage_in(ctx, SCR_IN1, flux_f, (size_t)n_faces) : nullptr;
     reset_dev_err(ctx);
     k_face_flux<<<nb(n_faces), 256, 0, s>>>(mesh->xyz.p, mesh->conn.p, mesh->n_nodes, mesh->n_elem, n_faces, df, dq,
-                                            flux, contrib.p, keys.p, ctx->dev_err.p);
+                                            flux, contrib, keys, ctx->dev_err.p);
     check_faces(ctx, "geo_apply_neumann_bcs");
-    k_iota32<<<nb(m), 256, 0, s>>>(idx.p, m);
+    k_iota32<<<nb(m), 256, 0, s>>>(idx, m);
     int bits = 1;
     while (bits < 31 && (int64_t(1) << bits) <= mesh->n_nodes) ++bits;
     size_t bytes = 0;
-    GEO_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.p, keys2.p, idx.p, idx2.p, m, 0, bits, s));
-    DevBuf<unsigned char> tmp(bytes + 16);
-    GEO_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, bytes, keys.p, keys2.p, idx.p, idx2.p, m, 0, bits, s));
+    GEO_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, keys2, idx, idx2, m, 0, bits, s));
+    unsigned char* tmp = ctx_scratch<unsigned char>(ctx, SCR_TMP2, bytes + 16);
+    GEO_CUDA(cub::DeviceRadixSort::SortPairs(tmp, bytes, keys, keys2, idx, idx2, m, 0, bits, s));
     double* dst = f;
     if (!is_device_ptr(f)) {
-        fd.alloc(n_f);
-        GEO_CUDA(cudaMemcpyAsync(fd.p, f, n_f * sizeof(double), cudaMemcpyHostToDevice, s));
-        dst = fd.p;
+        dst = ctx_scratch<double>(ctx, SCR_OUT0, (size_t)n_f);
+        GEO_CUDA(cudaMemcpyAsync(dst, f, n_f * sizeof(double), cudaMemcpyHostToDevice, s));
     }
-    k_run_sums<<<nb(m), 256, 0, s>>>(keys2.p, idx2.p, contrib.p, m, n_f, dst, ctx->dev_err.p);
+    k_run_sums<<<nb(m), 256, 0, s>>>(keys2, idx2, contrib, m, n_f, dst, ctx->dev_err.p);
     check_faces(ctx, "geo_apply_neumann_bcs");
     if (dst != f) copy_out(f, dst, (size_t)n_f, s);
     sync(ctx, "geo_apply_neumann_bcs");

@@ -7,6 +7,11 @@
 
 #include "common.cuh"
 
+namespace geo {
+// Slots of a context's scratch: one per temporary that a single call keeps live.
+enum ScratchSlot : int { SCR_IN0, SCR_IN1, SCR_IN2, SCR_OUT0, SCR_OUT1, SCR_TMP0, SCR_TMP1, SCR_TMP2, kScratchSlots };
+}  // namespace geo
+
 struct geo_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -14,6 +19,14 @@ struct geo_ctx {
     std::string err;
     geo::DevBuf<int> dev_err;  // [0]: DEV_ERR_* bits of element kernels
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Grow-only scratch for the temporaries of the entry points that run every
+    // step (staged inputs, per-element arrays, VTU offsets and chunks), and two
+    // pinned host buffers. Calls on one context run in order on its stream, so a
+    // slot is reused from call to call with no cudaMalloc or cudaFree: cudaFree
+    // synchronises the device, and in processes holding several GB it stalled
+    // single calls for up to a second. Held until the context is destroyed.
+    geo::DevBuf<unsigned char> scratch[geo::kScratchSlots];
+    geo::HostBuf<char> pinned[2];
 };
 
 struct geo_mesh {
@@ -66,6 +79,23 @@ void sync(geo_ctx* ctx, const char* what);
 void reset_dev_err(geo_ctx* ctx);
 int read_dev_err(geo_ctx* ctx);
 void raise_dev_err(geo_ctx* ctx, int bits, const char* what);
+
+// Slot `slot` of the context scratch, holding at least n values of T (contents undefined).
+template <class T>
+T* ctx_scratch(geo_ctx* ctx, int slot, size_t n) {
+    ctx->scratch[slot].ensure((n ? n : 1) * sizeof(T));
+    return reinterpret_cast<T*>(ctx->scratch[slot].p);
+}
+
+// src itself when it is device memory, else a copy in scratch slot `slot` (async on the context stream).
+template <class T>
+const T* stage_in(geo_ctx* ctx, int slot, const T* src, size_t n) {
+    if (n == 0) return nullptr;
+    if (is_device_ptr(src)) return src;
+    T* d = ctx_scratch<T>(ctx, slot, n);
+    GEO_CUDA(cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return d;
+}
 
 // assembly.cu
 void ensure_inverse_map(geo_mesh* m);

@@ -165,14 +165,14 @@ void check_material(double E, double nu, double mu) {
 void history_force(geo_ctx* ctx, geo_mesh* m, const double* stress, double* f_dev) {
     cudaStream_t s = ctx->stream;
     ensure_inverse_map(m);
-    DevBuf<double> ts, fe(30 * m->n_elem);
-    const double* ds = stage_in(stress, (size_t)(6 * m->n_elem), ts, s);
+    double* fe = ctx_scratch<double>(ctx, SCR_TMP0, (size_t)(30 * m->n_elem));
+    const double* ds = stage_in(ctx, SCR_IN0, stress, (size_t)(6 * m->n_elem));
     reset_dev_err(ctx);
-    k_maxwell_force<<<nb(m->n_elem), 128, 0, s>>>(m->xyz.p, m->conn.p, m->n_nodes, m->n_elem, ds, fe.p,
+    k_maxwell_force<<<nb(m->n_elem), 128, 0, s>>>(m->xyz.p, m->conn.p, m->n_nodes, m->n_elem, ds, fe,
                                                   ctx->dev_err.p);
     check_launch(ctx, "k_maxwell_force");
     raise_dev_err(ctx, read_dev_err(ctx), "maxwell history force");
-    k_gather3<<<nb(3 * m->n_nodes, 256), 256, 0, s>>>(m->inc_ptr.p, m->inc.p, fe.p, m->n_nodes, f_dev);
+    k_gather3<<<nb(3 * m->n_nodes, 256), 256, 0, s>>>(m->inc_ptr.p, m->inc.p, fe, m->n_nodes, f_dev);
     check_launch(ctx, "k_gather3");
 }
 
@@ -187,9 +187,9 @@ int geo_maxwell_history_force(geo_ctx* ctx, const geo_mesh* mesh, const double* 
     GEO_API_BEGIN(ctx)
     GEO_CHECK_ARG(ctx && mesh && stress && f, "NULL argument");
     geo_mesh* m = const_cast<geo_mesh*>(mesh);
-    DevBuf<double> out(3 * m->n_nodes);
-    history_force(ctx, m, stress, out.p);
-    copy_out(f, out.p, (size_t)(3 * m->n_nodes), ctx->stream);
+    double* out = ctx_scratch<double>(ctx, SCR_OUT0, (size_t)(3 * m->n_nodes));
+    history_force(ctx, m, stress, out);
+    copy_out(f, out, (size_t)(3 * m->n_nodes), ctx->stream);
     sync(ctx, "geo_maxwell_history_force");
     GEO_API_END
 }
@@ -204,9 +204,9 @@ int geo_assemble_maxwell_viscoelastic(geo_ctx* ctx, const geo_mesh* mesh, const 
     const int rc = geo_assemble_elasticity_stiffness(ctx, mesh, dofs, nullptr, E, nu, K);
     if (rc != GEO_OK) return rc;
     geo_mesh* m = const_cast<geo_mesh*>(mesh);
-    DevBuf<double> out(3 * m->n_nodes);
-    history_force(ctx, m, stress, out.p);
-    copy_out(f_history, out.p, (size_t)(3 * m->n_nodes), ctx->stream);
+    double* out = ctx_scratch<double>(ctx, SCR_OUT0, (size_t)(3 * m->n_nodes));
+    history_force(ctx, m, stress, out);
+    copy_out(f_history, out, (size_t)(3 * m->n_nodes), ctx->stream);
     sync(ctx, "geo_assemble_maxwell_viscoelastic");
     GEO_API_END
 }
@@ -220,19 +220,19 @@ int geo_update_stresses_maxwell(geo_ctx* ctx, const geo_mesh* mesh, double E, do
     GEO_CHECK_ARG(dt >= 0.0, "time step must be >= 0");
     cudaStream_t s = ctx->stream;
     const int64_t n = 3 * mesh->n_nodes, ne = mesh->n_elem;
-    DevBuf<double> t0, t1, t2, out(6 * ne);
-    const double* dun = stage_in(u_n, (size_t)n, t0, s);
-    const double* dunx = stage_in(u_next, (size_t)n, t1, s);
-    const double* dsn = stage_in(stress_n, (size_t)(6 * ne), t2, s);
+    double* out = ctx_scratch<double>(ctx, SCR_OUT0, (size_t)(6 * ne));
+    const double* dun = stage_in(ctx, SCR_IN0, u_n, (size_t)n);
+    const double* dunx = stage_in(ctx, SCR_IN1, u_next, (size_t)n);
+    const double* dsn = stage_in(ctx, SCR_IN2, stress_n, (size_t)(6 * ne));
     const double G = E / (2.0 * (1.0 + nu));
     const double tau = mu / G;
     const double lam = E / (3.0 * (1.0 - 2.0 * nu)) - 2.0 * G / 3.0;
     reset_dev_err(ctx);
     k_maxwell_update<<<nb(ne), 128, 0, s>>>(mesh->xyz.p, mesh->conn.p, mesh->n_nodes, ne, G, lam,
-                                            1.0 / (1.0 + dt / tau), dun, dunx, dsn, out.p, ctx->dev_err.p);
+                                            1.0 / (1.0 + dt / tau), dun, dunx, dsn, out, ctx->dev_err.p);
     check_launch(ctx, "k_maxwell_update");
     raise_dev_err(ctx, read_dev_err(ctx), "maxwell stress update");
-    copy_out(stress_next, out.p, (size_t)(6 * ne), s);
+    copy_out(stress_next, out, (size_t)(6 * ne), s);
     sync(ctx, "geo_update_stresses_maxwell");
     GEO_API_END
 }

@@ -168,7 +168,7 @@ __global__ void k_fill_iota_offsets(int64_t* off, int64_t n, int64_t stride) {
 // ------------------------------------------------------------------ host side
 struct FieldIn {
     std::string name;
-    const double* data;  // device
+    const double* data;  // host or device, as the caller passed it
     int64_t count;
     int comps;
 };
@@ -185,6 +185,11 @@ public:
     }
 
     int64_t pos() const { return pos_; }
+    // a field's values on the device (host data copied into the context scratch)
+    const double* stage(const double* data, size_t n) {
+        if (mode_ == TO_FILE) flush_pending();
+        return stage_in(ctx_, SCR_IN0, data, n);
+    }
     // true when the output did not fit the buffer (the size is still counted)
     bool overflow() const { return overflow_; }
 
@@ -202,26 +207,28 @@ public:
     template <class Item>
     void section(const Item& it, int64_t n, int fixed = 0) {
         if (n <= 0) return;
-        off_.ensure((size_t)n + 1);
+        // the previous section's chunks must have left the staging buffers first
+        if (mode_ == TO_FILE) flush_pending();
+        int64_t* off = ctx_scratch<int64_t>(ctx_, SCR_TMP1, (size_t)n + 1);
         const unsigned grid = blocks(n, 256);
         int64_t max_len = fixed;
         if (fixed) {
-            k_fill_iota_offsets<<<grid, 256, 0, s_>>>(off_.p, n, fixed);
+            k_fill_iota_offsets<<<grid, 256, 0, s_>>>(off, n, fixed);
             check_launch(ctx_, "k_fill_iota_offsets");
         } else {
-            len_.ensure((size_t)n + 1);
-            umax_.ensure(1);
-            GEO_CUDA(cudaMemsetAsync(umax_.p, 0, sizeof(unsigned long long), s_));
-            GEO_CUDA(cudaMemsetAsync(len_.p + n, 0, sizeof(int64_t), s_));
-            k_item_lengths<<<grid, 256, 0, s_>>>(it, n, len_.p, umax_.p);
+            int64_t* len = ctx_scratch<int64_t>(ctx_, SCR_TMP0, (size_t)n + 1);
+            unsigned long long* umax = ctx_scratch<unsigned long long>(ctx_, SCR_OUT1, 1);
+            GEO_CUDA(cudaMemsetAsync(umax, 0, sizeof(unsigned long long), s_));
+            GEO_CUDA(cudaMemsetAsync(len + n, 0, sizeof(int64_t), s_));
+            k_item_lengths<<<grid, 256, 0, s_>>>(it, n, len, umax);
             check_launch(ctx_, "k_item_lengths");
             size_t tmp_bytes = 0;
-            GEO_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, len_.p, off_.p, n + 1, s_));
-            scan_tmp_.ensure(tmp_bytes);
-            GEO_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp_.p, tmp_bytes, len_.p, off_.p, n + 1, s_));
-            GEO_CUDA(cudaMemcpyAsync(host_.m, umax_.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
+            GEO_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, len, off, n + 1, s_));
+            unsigned char* tmp = ctx_scratch<unsigned char>(ctx_, SCR_TMP2, tmp_bytes);
+            GEO_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, len, off, n + 1, s_));
+            GEO_CUDA(cudaMemcpyAsync(host_.m, umax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
         }
-        GEO_CUDA(cudaMemcpyAsync(&host_.total, off_.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+        GEO_CUDA(cudaMemcpyAsync(&host_.total, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
         GEO_CUDA(cudaStreamSynchronize(s_));
         if (!fixed) max_len = (int64_t)host_.m[0];
         const int64_t total = host_.total;
@@ -231,7 +238,7 @@ public:
             return;
         }
         if (mode_ == TO_DEVICE) {
-            k_item_write<<<blocks(n, kItemsPerBlock), kItemsPerBlock, 0, s_>>>(it, 0, n, off_.p, -pos_, out_);
+            k_item_write<<<blocks(n, kItemsPerBlock), kItemsPerBlock, 0, s_>>>(it, 0, n, off, -pos_, out_);
             check_launch(ctx_, "k_item_write");
             pos_ += total;
             return;
@@ -240,7 +247,7 @@ public:
         const int64_t m = std::max<int64_t>(1, kChunkBytes / std::max<int64_t>(1, max_len));
         const int64_t nchunks = cdiv(n, m);
         std::vector<int64_t> bounds((size_t)nchunks + 1);
-        GEO_CUDA(cudaMemcpy2DAsync(bounds.data(), sizeof(int64_t), off_.p, (size_t)m * sizeof(int64_t),
+        GEO_CUDA(cudaMemcpy2DAsync(bounds.data(), sizeof(int64_t), off, (size_t)m * sizeof(int64_t),
                                    sizeof(int64_t), (size_t)nchunks, cudaMemcpyDeviceToHost, s_));
         GEO_CUDA(cudaStreamSynchronize(s_));
         bounds[(size_t)nchunks] = total;
@@ -249,16 +256,16 @@ public:
             const int64_t bytes = bounds[(size_t)c + 1] - bounds[(size_t)c];
             const int slot = slot_;
             if (mode_ == TO_FILE) wait_slot(slot);
-            dstage_[slot].ensure((size_t)std::max<int64_t>(bytes, 16));
-            k_item_write<<<blocks(b - a, kItemsPerBlock), kItemsPerBlock, 0, s_>>>(it, a, b, off_.p,
-                                                                                  bounds[(size_t)c], dstage_[slot].p);
+            char* dst = ctx_scratch<char>(ctx_, slot ? SCR_IN1 : SCR_OUT0, stage_size(bytes));
+            k_item_write<<<blocks(b - a, kItemsPerBlock), kItemsPerBlock, 0, s_>>>(it, a, b, off,
+                                                                                  bounds[(size_t)c], dst);
             check_launch(ctx_, "k_item_write");
             if (mode_ == TO_HOST) {
-                GEO_CUDA(cudaMemcpyAsync(out_ + pos_, dstage_[slot].p, (size_t)bytes, cudaMemcpyDeviceToHost, s_));
+                GEO_CUDA(cudaMemcpyAsync(out_ + pos_, dst, (size_t)bytes, cudaMemcpyDeviceToHost, s_));
                 GEO_CUDA(cudaStreamSynchronize(s_));
             } else {
-                hstage_[slot].ensure((size_t)std::max<int64_t>(bytes, 16));
-                GEO_CUDA(cudaMemcpyAsync(hstage_[slot].p, dstage_[slot].p, (size_t)bytes, cudaMemcpyDeviceToHost, s_));
+                ctx_->pinned[slot].ensure(stage_size(bytes));
+                GEO_CUDA(cudaMemcpyAsync(ctx_->pinned[slot].p, dst, (size_t)bytes, cudaMemcpyDeviceToHost, s_));
                 if (!ev_[slot]) GEO_CUDA(cudaEventCreateWithFlags(&ev_[slot], cudaEventDisableTiming));
                 GEO_CUDA(cudaEventRecord(ev_[slot], s_));
                 pending_[slot] = bytes;
@@ -292,6 +299,12 @@ private:
         const int64_t cap = (int64_t)ctx_->sm_count * 16;
         return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, bs), cap));
     }
+    // staging sizes grow in powers of two from 1 MB, so the context's buffers settle
+    static size_t stage_size(int64_t bytes) {
+        size_t s = size_t(1) << 20;
+        while ((int64_t)s < bytes) s <<= 1;
+        return s;
+    }
     void put(const char* p, size_t n) {
         if (n && std::fwrite(p, 1, n, fp_) != n) fail(GEO_ERR_INVALID_ARG, "write to the output file failed");
     }
@@ -302,7 +315,7 @@ private:
         const int other = slot ^ 1;
         if (pending_[other] && order_[other] < order_[slot]) wait_slot(other);
         GEO_CUDA(cudaEventSynchronize(ev_[slot]));
-        put(hstage_[slot].p, (size_t)pending_[slot]);
+        put(ctx_->pinned[slot].p, (size_t)pending_[slot]);
         pending_[slot] = 0;
     }
     void flush_pending() {
@@ -323,11 +336,6 @@ private:
         unsigned long long m[1];
         int64_t total;
     } host_{};
-    DevBuf<int64_t> len_, off_;
-    DevBuf<unsigned long long> umax_;
-    DevBuf<unsigned char> scan_tmp_;
-    DevBuf<char> dstage_[2];
-    HostBuf<char> hstage_[2];
     cudaEvent_t ev_[2] = {nullptr, nullptr};
     int64_t pending_[2] = {0, 0};
     int64_t order_[2] = {0, 0};
@@ -343,7 +351,7 @@ void emit_fields(Emitter& em, const std::vector<FieldIn>& fields) {
             em.text("        <DataArray type=\"Float64\" Name=\"" + f.name +
                     (vec ? "\" NumberOfComponents=\"3\" format=\"ascii\">\n" : "\" format=\"ascii\">\n") +
                     "          ");
-            em.section(ValuesItem{f.data, f.comps}, f.count);
+            em.section(ValuesItem{em.stage(f.data, (size_t)(f.count * f.comps)), f.comps}, f.count);
             em.text("\n        </DataArray>\n");
         }
 }
@@ -391,18 +399,14 @@ void emit_vtu(Emitter& em, const geo_mesh* m, const std::vector<FieldIn>& pf, co
     em.finish();
 }
 
-std::vector<FieldIn> stage_fields(const geo_vtu_field* f, int32_t n, std::vector<DevBuf<double>>& keep,
-                                  cudaStream_t s) {
+std::vector<FieldIn> check_fields(const geo_vtu_field* f, int32_t n) {
     GEO_CHECK_ARG(n >= 0 && (n == 0 || f), "fields array is NULL");
     std::vector<FieldIn> out;
     for (int32_t i = 0; i < n; ++i) {
         GEO_CHECK_ARG(f[i].name, "field name is NULL");
         GEO_CHECK_ARG(f[i].components == 1 || f[i].components == 3, "field components must be 1 or 3");
         GEO_CHECK_ARG(f[i].count >= 0 && (f[i].count == 0 || f[i].data), "field data is NULL");
-        keep.emplace_back();
-        const double* d = f[i].count ? stage_in(f[i].data, (size_t)(f[i].count * f[i].components), keep.back(), s)
-                                     : nullptr;
-        out.push_back(FieldIn{f[i].name, d, f[i].count, f[i].components});
+        out.push_back(FieldIn{f[i].name, f[i].data, f[i].count, f[i].components});
     }
     return out;
 }
@@ -418,9 +422,8 @@ int geo_vtu_render(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* poin
                    const geo_vtu_field* cell_fields, int32_t n_cell, char* out, int64_t capacity, int64_t* size) {
     GEO_API_BEGIN(ctx)
     GEO_CHECK_ARG(ctx && mesh && size, "ctx/mesh/size is NULL");
-    std::vector<DevBuf<double>> keep;
-    const auto pf = stage_fields(point_fields, n_point, keep, ctx->stream);
-    const auto cf = stage_fields(cell_fields, n_cell, keep, ctx->stream);
+    const auto pf = check_fields(point_fields, n_point);
+    const auto cf = check_fields(cell_fields, n_cell);
     Emitter em(ctx, out ? (is_device_ptr(out) ? TO_DEVICE : TO_HOST) : SIZE_ONLY, out, out ? capacity : 0, nullptr);
     emit_vtu(em, mesh, pf, cf);
     *size = em.pos();
@@ -432,9 +435,8 @@ int geo_write_vtu(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point
                   const geo_vtu_field* cell_fields, int32_t n_cell, const char* path, int64_t* size) {
     GEO_API_BEGIN(ctx)
     GEO_CHECK_ARG(ctx && mesh && path, "ctx/mesh/path is NULL");
-    std::vector<DevBuf<double>> keep;
-    const auto pf = stage_fields(point_fields, n_point, keep, ctx->stream);
-    const auto cf = stage_fields(cell_fields, n_cell, keep, ctx->stream);
+    const auto pf = check_fields(point_fields, n_point);
+    const auto cf = check_fields(cell_fields, n_cell);
     FILE* fp = std::fopen(path, "wb");
     if (!fp) fail(GEO_ERR_INVALID_ARG, std::string("cannot create ") + path);
     try {
