@@ -403,6 +403,7 @@ struct geo_op {
     geo::DevBuf<int32_t> pfa, fids;
     geo::DevBuf<uint8_t> fflags;
     int max_for = 0;
+    int max_own = 0;  // largest own-node count of a patch
     // per-patch bound of the fixed-point scatter (Scatter in mf_kernels.cuh)
     geo::DevBuf<int32_t> pmaxinc;
     geo::DevBuf<float> pbound32;
@@ -420,6 +421,8 @@ struct geo_op {
     geo::PcgState* h_state = nullptr;  // pinned mirror
     int patch_grid[2] = {0, 0};        // resident patch-kernel blocks (FP64, FP32)
     int nbuf[2] = {2, 2};              // element-data buffers of the patch kernel (FP64, FP32)
+    int own_bulk[2] = {0, 0};          // own-node slices by bulk copy (FP32 thermal PCG), see setup
+    size_t patch_smem[2] = {0, 0};     // dynamic shared memory of the patch kernel
     int node_grid[2] = {0, 0};  // resident node-kernel blocks (FP64, mixed)
     // CUDA graphs of PCG iteration chunks, keyed by precision
     cudaGraphExec_t chunk[2] = {nullptr, nullptr};
@@ -464,15 +467,19 @@ PatchView view(const geo_op* op) {
     v.fids = op->fids.p;
     v.fflags = op->fflags.p;
     v.max_for = op->max_for;
+    v.max_own = op->max_own;
+    v.own_bulk = 0;
     return v;
 }
 
 // dynamic shared memory of the patch kernel: barriers, element-data buffers, node tables
 template <class K, class T>
-size_t smem_bytes(const geo_op* op, int nbuf) {
-    // xs (T), fixed-point accumulators (Scatter<T>::kWords INT32 words), node ids, flags
+size_t smem_bytes(const geo_op* op, int nbuf, bool own) {
+    // xs (T), fixed-point accumulators (Scatter<T>::kWords INT32 words), flags, and for
+    // FP32 thermal PCG the own-node slices
     const size_t tables = (size_t)op->max_local * K::DPN * (sizeof(T) + 4 * Scatter<T>::kWords) +
-                          (size_t)op->max_local * 5 + 16;
+                          (size_t)op->max_local + 16 +
+                          (own ? (size_t)own_bytes(op->max_own) : 0);
     return (nbuf == 2 ? patch_smem_tables<K, T, 2>(op->max_for) : patch_smem_tables<K, T, 1>(op->max_for)) + tables;
 }
 
@@ -491,39 +498,59 @@ void with_kernels(const geo_op* op, F&& f) {
 }
 
 template <class K, class T, int NBUF>
-int setup_patch_nbuf(geo_ctx* ctx, size_t bytes) {
+int setup_patch_nbuf(size_t attr_bytes, size_t plain, size_t own, int& per_sm_plain) {
     GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_FREE, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bytes));
+                                  (int)attr_bytes));
     GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_LIFT, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bytes));
+                                  (int)attr_bytes));
     GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_PCG, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bytes));
-    int per_sm = 0;
-    GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_patch<K, T, MODE_PCG, NBUF>, kPatchBS, bytes));
-    if (per_sm < 1) fail(GEO_ERR_UNSUPPORTED, "patch kernel does not fit on an SM");
-    return per_sm * ctx->sm_count;
+                                  (int)attr_bytes));
+    per_sm_plain = 0;
+    GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_plain, k_patch<K, T, MODE_PCG, NBUF>, kPatchBS,
+                                                           plain));
+    int per_sm_own = 0;
+    if (own)
+        GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_own, k_patch<K, T, MODE_PCG, NBUF>,
+                                                               kPatchBS, own));
+    return per_sm_own;
 }
 
-// Picks double buffering when it fits in shared memory; returns the resident grid.
+// Picks double buffering when it fits in shared memory, and the own-node bulk copies
+// (FP32 thermal PCG) when they cost no resident block: the gather then reads the
+// patch's own-node D^-1, r and p_old from shared memory, but their buffer (about 13
+// bytes per own node) took one block per SM away on meshes whose patches hold more
+// nodes, which was slower than the plain gather (80^3, 112^3). Returns the grid.
 template <class K, class T>
 int setup_patch_kernels(geo_op* op, int slot) {
-    if (smem_bytes<K, T>(op, 2) <= kSmemLimit) {
-        op->nbuf[slot] = 2;
-        return setup_patch_nbuf<K, T, 2>(op->ctx, smem_bytes<K, T>(op, 2));
+    int nbuf = 2;
+    if (smem_bytes<K, T>(op, 2, false) > kSmemLimit) {
+        if (smem_bytes<K, T>(op, 1, false) > kSmemLimit)
+            fail(GEO_ERR_UNSUPPORTED, "patch tables exceed shared memory (too many nodes per patch)");
+        nbuf = 1;
     }
-    if (smem_bytes<K, T>(op, 1) > kSmemLimit)
-        fail(GEO_ERR_UNSUPPORTED, "patch tables exceed shared memory (too many nodes per patch)");
-    op->nbuf[slot] = 1;
-    return setup_patch_nbuf<K, T, 1>(op->ctx, smem_bytes<K, T>(op, 1));
+    op->nbuf[slot] = nbuf;
+    const size_t plain = smem_bytes<K, T>(op, nbuf, false);
+    size_t own = own_bulk<K, T, MODE_PCG>() ? smem_bytes<K, T>(op, nbuf, true) : 0;
+    if (own > kSmemLimit) own = 0;
+    int per_sm = 0;
+    const int per_sm_own = nbuf == 2 ? setup_patch_nbuf<K, T, 2>(std::max(plain, own), plain, own, per_sm)
+                                     : setup_patch_nbuf<K, T, 1>(std::max(plain, own), plain, own, per_sm);
+    op->own_bulk[slot] = own && per_sm_own >= per_sm;
+    op->patch_smem[slot] = op->own_bulk[slot] ? own : plain;
+    if (per_sm < 1) fail(GEO_ERR_UNSUPPORTED, "patch kernel does not fit on an SM");
+    return per_sm * op->ctx->sm_count;
 }
 
 template <class K, class T, int MODE>
 void launch_patch(const geo_op* op, int slot, cudaStream_t s, const T* qd, const PatchArgs<T>& pa) {
     const unsigned g = (unsigned)std::min(op->patch_grid[slot], op->n_patches);
+    PatchView v = view(op);
+    v.own_bulk = op->own_bulk[slot];
+    const size_t smem = op->patch_smem[slot];
     if (op->nbuf[slot] == 2)
-        k_patch<K, T, MODE, 2><<<g, kPatchBS, smem_bytes<K, T>(op, 2), s>>>(view(op), qd, (T)op->cl, (T)op->cm, pa);
+        k_patch<K, T, MODE, 2><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
     else
-        k_patch<K, T, MODE, 1><<<g, kPatchBS, smem_bytes<K, T>(op, 1), s>>>(view(op), qd, (T)op->cl, (T)op->cm, pa);
+        k_patch<K, T, MODE, 1><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
 }
 
 // Recomputes qdata, diagonal, char_diag and the Jacobi inverse from op->coef.
@@ -579,7 +606,8 @@ void refresh_coefficients(geo_op* op) {
     std::memcpy(&maxd, &bits, sizeof(double));
     op->cd = maxd > 1.0 ? maxd : 1.0;  // assembly.rs:184-193
     op->dinv64.ensure(op->ndof);
-    op->dinv32.ensure(op->ndof);
+    // padded to whole 64-entry blocks: the patch kernel copies ranges rounded outwards to 4 values
+    op->dinv32.ensure((size_t)(op->ndof + 63) / 64 * 64);
     op->diag_new.ensure(op->ndof);
     k_dinv<<<nblk(op->ndof), 256, 0, s>>>(op->nperm.p, op->flags.p, op->dpn, op->N, op->diag_orig.p, op->cd,
                                          op->dinv64.p, op->dinv32.p, op->diag_new.p);
@@ -633,7 +661,9 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
     op->lc = std::move(L.lc);
     op->mask_orig.alloc(op->ndof);
     GEO_CUDA(cudaMemcpyAsync(op->mask_orig.p, dofs->mask.p, op->ndof, cudaMemcpyDeviceToDevice, s));
-    op->flags.alloc(op->N);
+    // padded to 16 bytes: the patch kernel copies flag ranges rounded outwards to 16
+    op->flags.alloc((size_t)(op->N + 15) / 16 * 16);
+    GEO_CUDA(cudaMemsetAsync(op->flags.p, 0, op->flags.bytes(), s));
     op->g_new.alloc(op->ndof);
     k_node_flags<<<nblk(op->N), 256, 0, s>>>(op->nperm.p, L.shared.p, dofs->mask.p, dofs->vals.p, dpn, op->N,
                                              op->flags.p, op->g_new.p);
@@ -641,8 +671,10 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
     sync(ctx, "operator layout");
     {
         const int P = op->n_patches;
-        std::vector<int32_t> pf(P + 1), pfa(P + 1);
+        std::vector<int32_t> pf(P + 1), pfa(P + 1), po(P + 1);
         GEO_CUDA(cudaMemcpy(pf.data(), op->pf.p, (P + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        GEO_CUDA(cudaMemcpy(po.data(), op->po.p, (P + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        for (int p = 0; p < P; ++p) op->max_own = std::max(op->max_own, po[p + 1] - po[p]);
         int64_t acc = 0;
         for (int p = 0; p < P; ++p) {
             const int nfor = pf[p + 1] - pf[p];

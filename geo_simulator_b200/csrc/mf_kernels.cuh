@@ -62,6 +62,8 @@ struct PatchView {
     const int32_t* fids;
     const uint8_t* fflags;
     int max_for;
+    int max_own;   // the largest own-node count of a patch
+    int own_bulk;  // own-node slices by bulk copy (FP32 thermal PCG; the launch's shared memory holds them)
 };
 
 // ------------------------------------------------------------------ shared-memory scatter
@@ -234,11 +236,22 @@ __host__ __device__ inline uint32_t patch_aux_bytes(int max_for) {
            round16((uint32_t)((max_for + kForeignAlign - 1) / kForeignAlign * kForeignAlign));
 }
 
-// shared memory layout: [2 mbarriers | NBUF x (lc | qd) | NBUF x (meta | foreign ids | foreign flags) |
-// xs | ys | node ids | flags]
+// Own-node slices (FP32 PCG, one DOF per node): D^-1, r and p_old of the patch's
+// own node range, and its flags, copied with cp.async.bulk from 16-byte aligned
+// starts (the range rounded outwards to 4 values / 16 flags). Capacities per array:
+__host__ __device__ inline uint32_t own_cap(int max_own) { return (uint32_t)(max_own + 8 + 3) & ~3u; }
+__host__ __device__ inline uint32_t own_capf(int max_own) { return (uint32_t)(max_own + 32 + 15) & ~15u; }
+__host__ __device__ inline uint32_t own_bytes(int max_own) { return 12u * own_cap(max_own) + own_capf(max_own); }
+template <class K, class T, int MODE>
+__host__ __device__ constexpr bool own_bulk() {
+    return MODE == MODE_PCG && K::DPN == 1 && sizeof(T) == 4;
+}
+
+// shared memory layout: [3 mbarriers (32 B) | NBUF x (lc | qd) | NBUF x (meta | foreign ids | foreign flags) |
+// xs | ys | flags | own-node slices (FP32 thermal)]
 template <class K, class T, int NBUF>
 __host__ __device__ constexpr size_t patch_smem_fixed() {
-    return 16 + (size_t)NBUF * (patch_bytes_lc<K, T>() + patch_bytes_qd<K, T>());
+    return 32 + (size_t)NBUF * (patch_bytes_lc<K, T>() + patch_bytes_qd<K, T>());
 }
 template <class K, class T, int NBUF>
 __host__ __device__ inline size_t patch_smem_tables(int max_for) {
@@ -251,18 +264,23 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     constexpr int DPN = K::DPN;
     constexpr uint32_t LCB = patch_bytes_lc<K, T>(), QDB = patch_bytes_qd<K, T>();
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
-    unsigned char* ebuf = smem + 16;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // [0..NBUF): element data; [2]: own-node slices
+    unsigned char* ebuf = smem + 32;
+    const bool OWNB = own_bulk<K, T, MODE>() && pv.own_bulk != 0;
     using SC = Scatter<T>;
     const int M = pv.max_local * DPN;  // DOF slots of the patch-local table
     unsigned char* abuf = smem + patch_smem_fixed<K, T, NBUF>();  // NBUF x (meta | ids | flags)
     const uint32_t AUX = patch_aux_bytes(pv.max_for), AIDS = patch_aux_ids(pv.max_for);
     T* xs = reinterpret_cast<T*>(smem + patch_smem_tables<K, T, NBUF>(pv.max_for));
     int* ys = reinterpret_cast<int*>(xs + M);  // fixed-point accumulators, SC::kWords x M words
-    int* snode = ys + SC::kWords * M;
     // FP32 scatter: per component, min and max of x over the patch as order keys, by patch parity
     __shared__ unsigned s_lo[2][DPN], s_hi[2][DPN];
-    uint8_t* sfl = reinterpret_cast<uint8_t*>(snode + pv.max_local);
+    uint8_t* sfl = reinterpret_cast<uint8_t*>(ys + SC::kWords * M);
+    const uint32_t OCAP = own_cap(pv.max_own);
+    float* own_d = reinterpret_cast<float*>(smem + (((size_t)(sfl + pv.max_local - smem) + 15) & ~(size_t)15));
+    float* own_r = own_d + OCAP;
+    float* own_p = own_r + OCAP;
+    uint8_t* own_f = reinterpret_cast<uint8_t*>(own_p + OCAP);
     T beta = T(0);
     const T* pold = nullptr;
     T* pnew = nullptr;
@@ -275,6 +293,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     }
     if (threadIdx.x == 0) {
         for (int b = 0; b < NBUF; ++b) mbar_init(&bar[b], 1);
+        if (OWNB) mbar_init(&bar[2], 1);
         mbar_fence_init();
         for (int c = 0; c < DPN; ++c) {
             s_lo[0][c] = s_lo[1][c] = 0xffffffffu;
@@ -304,16 +323,37 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             bulk_g2s(ab + sizeof(PatchMeta) + AIDS, pv.fflags + m.fa, fb, &bar[b]);
         }
     };
-    if (threadIdx.x == 0 && blockIdx.x < pv.n_patches) issue(blockIdx.x, 0);
-    uint32_t phase = 0;  // bit b = parity of buffer b
+    // thread 0: D^-1, r, p_old and flags of the patch's own nodes (single buffer, bar[2])
+    auto issue_own = [&](int patch) {
+        const int o0 = pv.po[patch], o1 = pv.po[patch + 1];
+        const int a0 = o0 & ~3, n4 = ((o1 + 3) & ~3) - a0;     // values, 16-byte aligned
+        const int f0 = o0 & ~15, nf = ((o1 + 15) & ~15) - f0;  // flags, 16-byte aligned
+        const uint32_t vb = (uint32_t)n4 * 4u;
+        mbar_expect_tx(&bar[2], 3u * vb + (uint32_t)nf);
+        if (n4) {
+            bulk_g2s(own_d, a.dinv + a0, vb, &bar[2]);
+            bulk_g2s(own_r, a.r + a0, vb, &bar[2]);
+            bulk_g2s(own_p, pold + a0, vb, &bar[2]);
+        }
+        if (nf) bulk_g2s(own_f, pv.flags + f0, (uint32_t)nf, &bar[2]);
+    };
+    if (threadIdx.x == 0 && blockIdx.x < pv.n_patches) {
+        issue(blockIdx.x, 0);
+        if (OWNB) issue_own(blockIdx.x);
+    }
+    uint32_t phase = 0;  // bit b = parity of buffer b; bit 2 = parity of the own-node buffer
     double dot = 0.0, pdd = 0.0;
     int k = 0;
     for (int patch = blockIdx.x; patch < pv.n_patches; patch += gridDim.x, ++k) {
         const int b = NBUF == 2 ? (k & 1) : 0;
         if (NBUF == 2 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, b ^ 1);
         // the patch's sizes, element data and foreign lists (copied during the previous patch)
-        const bool ok = mbar_wait(&bar[b], (phase >> b) & 1);
+        bool ok = mbar_wait(&bar[b], (phase >> b) & 1);
         phase ^= 1u << b;
+        if (OWNB) {
+            ok = mbar_wait(&bar[2], (phase >> 2) & 1) && ok;
+            phase ^= 4u;
+        }
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicOr(a.err, DEV_ERR_TIMEOUT);
             return;
@@ -344,7 +384,12 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
 #pragma unroll
             for (int g = 0; g < kGather; ++g) {
                 const int u = u0 + g * blockDim.x;
-                if (u < nloc) {
+                if (OWNB && u < nown) {  // from the own-node slices in shared memory
+                    fl[g] = own_f[(o0 & 15) + u];
+                    d0[g][0] = own_d[(o0 & 3) + u];
+                    d1[g][0] = own_r[(o0 & 3) + u];
+                    d2[g][0] = own_p[(o0 & 3) + u];
+                } else if (u < nloc) {
                     fl[g] = u < nown ? pv.flags[node[g]] : sffl[u - nown];
 #pragma unroll
                     for (int c = 0; c < DPN; ++c) {
@@ -363,7 +408,6 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             for (int g = 0; g < kGather; ++g) {
                 const int u = u0 + g * blockDim.x;
                 if (u >= nloc) continue;
-                snode[u] = node[g];
                 sfl[u] = fl[g];
 #pragma unroll
                 for (int c = 0; c < DPN; ++c) {
@@ -399,6 +443,8 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             }
         }
         __syncthreads();
+        // the own-node buffer is free again: bring the next patch's slices during steps 2 and 3
+        if (OWNB && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue_own(patch + gridDim.x);
         // 2. elements, scattered as fixed-point integers with scale S (see Scatter)
         T S = T(1), invS = T(1);
         {
@@ -449,10 +495,9 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                 for (int c = 0; c < DPN; ++c) SC::add(ys, M, li[l] * DPN + c, ye[l * DPN + c] * S);
         }
         __syncthreads();
-        if (NBUF == 1 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, 0);
-        // 3. flush
+        // 3. flush (node ids: the own range, then the foreign list still in the aux buffer)
         for (int u = threadIdx.x; u < nloc; u += blockDim.x) {
-            const int node = snode[u];
+            const int node = u < nown ? o0 + u : sfor[u - nown];
             const uint8_t fl = sfl[u];
             const bool plain = u < nown && !(fl & kFlagShared);
 #pragma unroll
@@ -465,6 +510,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             }
         }
         __syncthreads();
+        if (NBUF == 1 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, 0);
     }
     if (MODE == MODE_PCG) {
         double v[2] = {dot, pdd};
