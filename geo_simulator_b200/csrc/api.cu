@@ -47,6 +47,18 @@ __global__ void aos_to_soa3(const double* __restrict__ aos, double* __restrict__
     }
 }
 
+// mask[i] = mask[i] != 0, and the count of ones added to *count
+__global__ void k_normalize_mask(uint8_t* __restrict__ mask, int64_t n, unsigned long long* __restrict__ count) {
+    unsigned c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t v = mask[i] ? 1 : 0;
+        mask[i] = v;
+        c += v;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
 __global__ void conn_to_soa(const int32_t* __restrict__ aos, int32_t* __restrict__ soa, int64_t E,
                             int64_t n_nodes, int* err) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
@@ -187,22 +199,24 @@ int geo_dofs_create(geo_ctx* ctx, int64_t n_nodes, int32_t dofs_per_node, const 
     d->dpn = dofs_per_node;
     d->n_dofs = n_nodes * dofs_per_node;
     GEO_CHECK_ARG(d->n_dofs < (int64_t(1) << 31), "too many DOFs");
-    d->h_mask.assign(d->n_dofs, 0);
-    d->h_vals.assign(d->n_dofs, 0.0);
-    if (mask)
-        GEO_CUDA(cudaMemcpy(d->h_mask.data(), mask, d->n_dofs, cudaMemcpyDefault));
-    if (values)
-        GEO_CUDA(cudaMemcpy(d->h_vals.data(), values, d->n_dofs * sizeof(double), cudaMemcpyDefault));
-    int64_t nd = 0;
-    for (int64_t i = 0; i < d->n_dofs; ++i) {
-        d->h_mask[i] = d->h_mask[i] ? 1 : 0;
-        nd += d->h_mask[i];
-    }
-    d->n_dir = nd;
+    // copied straight to the device (DMA from pinned callers' buffers); the mask is
+    // normalised to 0/1 and its Dirichlet DOFs counted there
+    cudaStream_t s = ctx->stream;
     d->mask.alloc(d->n_dofs);
     d->vals.alloc(d->n_dofs);
-    GEO_CUDA(cudaMemcpy(d->mask.p, d->h_mask.data(), d->n_dofs, cudaMemcpyHostToDevice));
-    GEO_CUDA(cudaMemcpy(d->vals.p, d->h_vals.data(), d->n_dofs * sizeof(double), cudaMemcpyHostToDevice));
+    if (mask) GEO_CUDA(cudaMemcpyAsync(d->mask.p, mask, d->n_dofs, cudaMemcpyDefault, s));
+    else GEO_CUDA(cudaMemsetAsync(d->mask.p, 0, d->n_dofs, s));
+    if (values) GEO_CUDA(cudaMemcpyAsync(d->vals.p, values, d->n_dofs * sizeof(double), cudaMemcpyDefault, s));
+    else GEO_CUDA(cudaMemsetAsync(d->vals.p, 0, d->n_dofs * sizeof(double), s));
+    unsigned long long* cnt = ctx_scratch<unsigned long long>(ctx, SCR_TMP0, 1);
+    GEO_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
+    k_normalize_mask<<<(unsigned)std::min<int64_t>(cdiv(d->n_dofs, 256), (int64_t)ctx->sm_count * 8), 256, 0, s>>>(
+        d->mask.p, d->n_dofs, cnt);
+    check_launch(ctx, "k_normalize_mask");
+    unsigned long long nd = 0;
+    GEO_CUDA(cudaMemcpyAsync(&nd, cnt, sizeof nd, cudaMemcpyDeviceToHost, s));
+    GEO_CUDA(cudaStreamSynchronize(s));
+    d->n_dir = (int64_t)nd;
     *out = d.release();
     GEO_API_END
 }

@@ -47,8 +47,6 @@ struct geo_dofs {
     geo_ctx* ctx = nullptr;
     int64_t n_nodes = 0, n_dofs = 0, n_dir = 0;
     int dpn = 1;
-    std::vector<uint8_t> h_mask;
-    std::vector<double> h_vals;
     geo::DevBuf<uint8_t> mask;
     geo::DevBuf<double> vals;
 };
