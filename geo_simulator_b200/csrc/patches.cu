@@ -1,7 +1,8 @@
 // GPU construction of the element-patch layout (see patches.h). All steps are
 // data-parallel: Morton keys + radix sort for the element order, atomicMin of
-// the first-touch position for the node order, one 64-bit key sort for the
-// per-patch foreign lists, binary searches for the local indices.
+// the first-touch position for the node order, a sort of each patch's own
+// candidates in shared memory (one block per patch) for the per-patch foreign
+// lists, binary searches for the local indices.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -123,38 +124,109 @@ __global__ void k_patch_bounds(const int32_t* __restrict__ ft_sorted, int64_t N,
 }
 
 // key = patch << 32 | new node for every foreign incidence, ~0 otherwise
-__global__ void k_foreign_keys(const int32_t* __restrict__ conn, const int32_t* __restrict__ eperm,
-                               const int32_t* __restrict__ ninv, const int32_t* __restrict__ po, int64_t E,
-                               uint64_t* __restrict__ key) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= E * 10) return;
-    const int64_t ne = t / 10;
-    const int l = (int)(t % 10);
-    const int32_t nn = ninv[conn[l * E + eperm[ne]]];
-    const int p = (int)(ne / kPatchElems);
-    key[t] = nn < po[p] ? ((uint64_t)p << 32 | (uint32_t)nn) : ~0ull;
-}
+// Foreign nodes of a patch: the distinct node ids below the patch's own range that
+// its elements reference, in ascending order. One block per patch gathers the
+// candidates of its (at most 10 * kPatchElems) incidences into shared memory,
+// sorts them there (bitonic network) and marks the first of every run of equal ids.
+constexpr int kForeignBS = 256;
+constexpr int kForeignCap = 4096;  // power of two >= 10 * kPatchElems
+static_assert(kForeignCap >= 10 * kPatchElems, "foreign candidate buffer too small");
 
-__global__ void k_foreign_bounds(const uint64_t* __restrict__ uniq, int64_t nf, int P, int32_t* __restrict__ pf) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p > P) return;
-    const uint64_t key = (uint64_t)p << 32;
-    int64_t lo = 0, hi = nf;
-    while (lo < hi) {
-        const int64_t m = (lo + hi) >> 1;
-        if (uniq[m] < key) lo = m + 1;
-        else hi = m;
+__device__ int patch_foreign_sorted(const int32_t* __restrict__ conn, const int32_t* __restrict__ eperm,
+                                    const int32_t* __restrict__ ninv, const int32_t* __restrict__ po, int64_t E,
+                                    int* s_keys) {
+    __shared__ int s_n;
+    const int p = blockIdx.x;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const int32_t own0 = po[p];
+    const int64_t e0 = (int64_t)p * kPatchElems, e1 = min(E, e0 + kPatchElems);
+    const int n_inc = (int)((e1 - e0) * 10);
+    for (int t = threadIdx.x; t < n_inc; t += blockDim.x) {
+        const int64_t ne = e0 + t / 10;
+        const int l = t % 10;
+        const int32_t nn = ninv[conn[(int64_t)l * E + eperm[ne]]];
+        if (nn < own0) s_keys[atomicAdd(&s_n, 1)] = nn;
     }
-    pf[p] = (int32_t)lo;
+    __syncthreads();
+    const int n = s_n;
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int i = n + threadIdx.x; i < m; i += blockDim.x) s_keys[i] = INT32_MAX;
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const int a = s_keys[i], b = s_keys[ixj];
+                    if (((i & k) == 0) ? (a > b) : (a < b)) {
+                        s_keys[i] = b;
+                        s_keys[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    return n;
 }
 
-__global__ void k_foreign_nodes(const uint64_t* __restrict__ uniq, int64_t nf, int32_t* __restrict__ foreign,
-                                uint8_t* __restrict__ shared) {
-    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (j >= nf) return;
-    const int32_t nn = (int32_t)(uniq[j] & 0xffffffffull);
-    foreign[j] = nn;
-    shared[nn] = 1;
+// Block-wide exclusive scan of one int per thread (blockDim.x == kForeignBS); total in *total.
+__device__ int block_exclusive_scan(int v, int* total) {
+    __shared__ int s_warp[kForeignBS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    int base = 0, sum = 0;
+    for (int w = 0; w < kForeignBS / 32; ++w) {
+        if (w < warp) base += s_warp[w];
+        sum += s_warp[w];
+    }
+    __syncthreads();
+    *total = sum;
+    return base + x - v;
+}
+
+// Pass 1 (write == false): cnt[p] = number of distinct foreign nodes of patch p.
+// Pass 2 (write == true): foreign[pf[p] ..] = those nodes in ascending order, shared[node] = 1.
+template <bool WRITE>
+__global__ void __launch_bounds__(kForeignBS) k_patch_foreign_lists(
+    const int32_t* __restrict__ conn, const int32_t* __restrict__ eperm, const int32_t* __restrict__ ninv,
+    const int32_t* __restrict__ po, int64_t E, int32_t* __restrict__ cnt, const int32_t* __restrict__ pf,
+    int32_t* __restrict__ foreign, uint8_t* __restrict__ shared) {
+    __shared__ int s_keys[kForeignCap];
+    const int n = patch_foreign_sorted(conn, eperm, ninv, po, E, s_keys);
+    // each thread takes a contiguous chunk of the sorted candidates
+    constexpr int kPer = kForeignCap / kForeignBS;
+    const int i0 = threadIdx.x * kPer;
+    int c = 0;
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const int i = i0 + q;
+        if (i < n && (i == 0 || s_keys[i] != s_keys[i - 1])) ++c;
+    }
+    int total = 0;
+    int at = block_exclusive_scan(c, &total);
+    if (!WRITE) {
+        if (threadIdx.x == 0) cnt[blockIdx.x] = total;
+        return;
+    }
+    const int32_t base = pf[blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const int i = i0 + q;
+        if (i < n && (i == 0 || s_keys[i] != s_keys[i - 1])) {
+            const int nn = s_keys[i];
+            foreign[base + at++] = nn;
+            shared[nn] = 1;
+        }
+    }
 }
 
 __global__ void k_local_conn(const int32_t* __restrict__ conn, const int32_t* __restrict__ eperm,
@@ -327,22 +399,22 @@ void build_patches(cudaStream_t s, int64_t N, const double* xyz, int64_t E, cons
     GEO_CUDA(cudaMemsetAsync(L.shared.p, 0, N, s));
     int64_t nf = 0;
     {
-        DevBuf<uint64_t> k0(E * 10), k1(E * 10);
-        k_foreign_keys<<<nb(E * 10), 256, 0, s>>>(conn, L.eperm.p, L.ninv.p, L.patch_own.p, E, k0.p);
+        // per patch in shared memory: count, offsets by scan, then the sorted lists
+        DevBuf<int32_t> cnt(P + 1);
+        GEO_CUDA(cudaMemsetAsync(cnt.p + P, 0, sizeof(int32_t), s));
+        k_patch_foreign_lists<false><<<(unsigned)P, kForeignBS, 0, s>>>(conn, L.eperm.p, L.ninv.p, L.patch_own.p, E,
+                                                                       cnt.p, nullptr, nullptr, nullptr);
         cub_call(s, [&](void* t, size_t& b) {
-            return cub::DeviceRadixSort::SortKeys(t, b, k0.p, k1.p, E * 10, 0, 64, s);
+            return cub::DeviceScan::ExclusiveSum(t, b, cnt.p, L.patch_foreign.p, P + 1, s);
         });
-        DevBuf<int64_t> nsel(1);
-        cub_call(s, [&](void* t, size_t& b) {
-            return cub::DeviceSelect::Unique(t, b, k1.p, k0.p, nsel.p, E * 10, s);
-        });
-        GEO_CUDA(cudaMemcpy(&nf, nsel.p, sizeof(int64_t), cudaMemcpyDeviceToHost));
-        uint64_t lastk = 0;
-        if (nf > 0) GEO_CUDA(cudaMemcpy(&lastk, k0.p + nf - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost));
-        if (nf > 0 && lastk == ~0ull) --nf;
+        int32_t total = 0;
+        GEO_CUDA(cudaMemcpy(&total, L.patch_foreign.p + P, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        nf = total;
         L.foreign.alloc(std::max<int64_t>(nf, 1));
-        k_foreign_bounds<<<nb(P + 1), 256, 0, s>>>(k0.p, nf, P, L.patch_foreign.p);
-        if (nf > 0) k_foreign_nodes<<<nb(nf), 256, 0, s>>>(k0.p, nf, L.foreign.p, L.shared.p);
+        k_patch_foreign_lists<true><<<(unsigned)P, kForeignBS, 0, s>>>(conn, L.eperm.p, L.ninv.p, L.patch_own.p, E,
+                                                                      nullptr, L.patch_foreign.p, L.foreign.p,
+                                                                      L.shared.p);
+        GEO_CUDA(cudaGetLastError());
         GEO_CUDA(cudaStreamSynchronize(s));
     }
     // ---- local connectivity and patch-table size
