@@ -342,20 +342,37 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         if (OWNB) issue_own(blockIdx.x);
     }
     uint32_t phase = 0;  // bit b = parity of buffer b; bit 2 = parity of the own-node buffer
+    // bit b: a copy into buffer b is in flight (tracked by thread 0, which issues them)
+    uint32_t pend = blockIdx.x < pv.n_patches ? (OWNB ? 5u : 1u) : 0u;
     double dot = 0.0, pdd = 0.0;
     int k = 0;
     for (int patch = blockIdx.x; patch < pv.n_patches; patch += gridDim.x, ++k) {
         const int b = NBUF == 2 ? (k & 1) : 0;
-        if (NBUF == 2 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, b ^ 1);
+        if (NBUF == 2 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) {
+            issue(patch + gridDim.x, b ^ 1);
+            pend |= 1u << (b ^ 1);
+        }
         // the patch's sizes, element data and foreign lists (copied during the previous patch)
         bool ok = mbar_wait(&bar[b], (phase >> b) & 1);
-        phase ^= 1u << b;
+        if (ok) {
+            phase ^= 1u << b;
+            pend &= ~(1u << b);
+        }
         if (OWNB) {
-            ok = mbar_wait(&bar[2], (phase >> 2) & 1) && ok;
-            phase ^= 4u;
+            const bool ok2 = mbar_wait(&bar[2], (phase >> 2) & 1);
+            if (ok2) {
+                phase ^= 4u;
+                pend &= ~4u;
+            }
+            ok = ok && ok2;
         }
         if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicOr(a.err, DEV_ERR_TIMEOUT);
+            if (threadIdx.x == 0) {
+                atomicOr(a.err, DEV_ERR_TIMEOUT);
+                // let copies still in flight land (bounded waits) before the block's shared memory is released
+                for (int q = 0; q < 3; ++q)
+                    if ((pend >> q) & 1) mbar_wait(&bar[q], (phase >> q) & 1);
+            }
             return;
         }
         const unsigned char* ab = abuf + (size_t)b * AUX;
@@ -444,7 +461,10 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         }
         __syncthreads();
         // the own-node buffer is free again: bring the next patch's slices during steps 2 and 3
-        if (OWNB && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue_own(patch + gridDim.x);
+        if (OWNB && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) {
+            issue_own(patch + gridDim.x);
+            pend |= 4u;
+        }
         // 2. elements, scattered as fixed-point integers with scale S (see Scatter)
         T S = T(1), invS = T(1);
         {
@@ -510,7 +530,10 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             }
         }
         __syncthreads();
-        if (NBUF == 1 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) issue(patch + gridDim.x, 0);
+        if (NBUF == 1 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) {
+            issue(patch + gridDim.x, 0);
+            pend |= 1u;
+        }
     }
     if (MODE == MODE_PCG) {
         double v[2] = {dot, pdd};
