@@ -14,7 +14,14 @@ namespace geo {
 namespace {
 
 constexpr int kBS = 256;
-constexpr int kVec = 8;  // lanes per CSR row
+#ifndef GEO_CSR_VEC
+#define GEO_CSR_VEC 8
+#endif
+#ifndef GEO_CSR_UNROLL
+#define GEO_CSR_UNROLL 4
+#endif
+constexpr int kVec = GEO_CSR_VEC;           // lanes per CSR row
+constexpr int kUnrollCsr = GEO_CSR_UNROLL;  // row entries in flight per lane in the SpMV
 
 struct CsrPcgArgs {
     const int64_t* indptr;
@@ -41,7 +48,7 @@ __device__ __forceinline__ int64_t lower_bound_i32(const int32_t* idx, int64_t b
     return b;
 }
 
-__global__ void __launch_bounds__(kBS) k_csr_pcg(CsrPcgArgs a) {
+__global__ void __launch_bounds__(kBS, 4) k_csr_pcg(CsrPcgArgs a) {
     const unsigned nb = gridDim.x;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t nth = (int64_t)gridDim.x * blockDim.x;
@@ -93,9 +100,26 @@ __global__ void __launch_bounds__(kBS) k_csr_pcg(CsrPcgArgs a) {
             for (int64_t rbase = warp * rows_per_warp; rbase < n; rbase += nwarps * rows_per_warp) {
                 const int64_t row = rbase + lane / kVec;
                 double s = 0.0;
-                if (row < n)
-                    for (int64_t pp = a.indptr[row] + sub; pp < a.indptr[row + 1]; pp += kVec)
-                        s += a.data[pp] * a.p[a.indices[pp]];
+                if (row < n) {
+                    // kUnroll entries per lane in flight: all value/index loads, then all
+                    // gathers of p, then the products in the original order (same sum)
+                    const int64_t re = __ldg(a.indptr + row + 1);
+                    for (int64_t pp0 = __ldg(a.indptr + row) + sub; pp0 < re; pp0 += kUnrollCsr * kVec) {
+                        double d[kUnrollCsr], pv[kUnrollCsr];
+                        int32_t c[kUnrollCsr];
+#pragma unroll
+                        for (int u = 0; u < kUnrollCsr; ++u) {
+                            const int64_t pp = pp0 + (int64_t)u * kVec;
+                            d[u] = pp < re ? __ldg(a.data + pp) : 0.0;
+                            c[u] = pp < re ? __ldg(a.indices + pp) : -1;
+                        }
+#pragma unroll
+                        for (int u = 0; u < kUnrollCsr; ++u) pv[u] = c[u] >= 0 ? a.p[c[u]] : 0.0;
+#pragma unroll
+                        for (int u = 0; u < kUnrollCsr; ++u)
+                            if (c[u] >= 0) s += d[u] * pv[u];
+                    }
+                }
 #pragma unroll
                 for (int o = kVec / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, kVec);
                 if (row < n && sub == 0) {
