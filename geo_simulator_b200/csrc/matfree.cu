@@ -479,7 +479,7 @@ size_t smem_bytes(const geo_op* op, int nbuf, bool own) {
     // FP32 thermal PCG the own-node slices
     const size_t tables = (size_t)op->max_local * K::DPN * (sizeof(T) + 4 * Scatter<T>::kWords) +
                           (size_t)op->max_local + 16 +
-                          (own ? (size_t)own_bytes(op->max_own) : 0);
+                          (own ? (size_t)own_bytes<T>(op->max_own, K::DPN) : 0);
     return (nbuf == 2 ? patch_smem_tables<K, T, 2>(op->max_for) : patch_smem_tables<K, T, 1>(op->max_for)) + tables;
 }
 
@@ -605,7 +605,8 @@ void refresh_coefficients(geo_op* op) {
     double maxd;
     std::memcpy(&maxd, &bits, sizeof(double));
     op->cd = maxd > 1.0 ? maxd : 1.0;  // assembly.rs:184-193
-    op->dinv64.ensure(op->ndof);
+    // padded to whole 64-entry blocks: the patch kernel copies ranges rounded outwards to 16 bytes
+    op->dinv64.ensure((size_t)(op->ndof + 63) / 64 * 64);
     // padded to whole 64-entry blocks: the patch kernel copies ranges rounded outwards to 4 values
     op->dinv32.ensure((size_t)(op->ndof + 63) / 64 * 64);
     op->diag_new.ensure(op->ndof);

@@ -236,15 +236,23 @@ __host__ __device__ inline uint32_t patch_aux_bytes(int max_for) {
            round16((uint32_t)((max_for + kForeignAlign - 1) / kForeignAlign * kForeignAlign));
 }
 
-// Own-node slices (FP32 PCG, one DOF per node): D^-1, r and p_old of the patch's
-// own node range, and its flags, copied with cp.async.bulk from 16-byte aligned
-// starts (the range rounded outwards to 4 values / 16 flags). Capacities per array:
-__host__ __device__ inline uint32_t own_cap(int max_own) { return (uint32_t)(max_own + 8 + 3) & ~3u; }
+// Own-node slices (PCG mode): D^-1, r and p_old over the patch's own DOF range
+// [dpn o0, dpn o1) (components interleaved, so the range is contiguous) and the
+// flags of its own nodes, copied with cp.async.bulk from 16-byte aligned starts
+// (ranges rounded outwards to 16 bytes). Capacities: values per array, flag bytes.
+template <class T>
+__host__ __device__ inline uint32_t own_cap(int max_own, int dpn) {
+    constexpr uint32_t V = 16 / sizeof(T);
+    return ((uint32_t)(max_own * dpn) + 2 * V + V - 1) & ~(V - 1);
+}
 __host__ __device__ inline uint32_t own_capf(int max_own) { return (uint32_t)(max_own + 32 + 15) & ~15u; }
-__host__ __device__ inline uint32_t own_bytes(int max_own) { return 12u * own_cap(max_own) + own_capf(max_own); }
+template <class T>
+__host__ __device__ inline uint32_t own_bytes(int max_own, int dpn) {
+    return 3u * own_cap<T>(max_own, dpn) * (uint32_t)sizeof(T) + own_capf(max_own);
+}
 template <class K, class T, int MODE>
 __host__ __device__ constexpr bool own_bulk() {
-    return MODE == MODE_PCG && K::DPN == 1 && sizeof(T) == 4;
+    return MODE == MODE_PCG;
 }
 
 // shared memory layout: [3 mbarriers (32 B) | NBUF x (lc | qd) | NBUF x (meta | foreign ids | foreign flags) |
@@ -276,10 +284,10 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     // FP32 scatter: per component, min and max of x over the patch as order keys, by patch parity
     __shared__ unsigned s_lo[2][DPN], s_hi[2][DPN];
     uint8_t* sfl = reinterpret_cast<uint8_t*>(ys + SC::kWords * M);
-    const uint32_t OCAP = own_cap(pv.max_own);
-    float* own_d = reinterpret_cast<float*>(smem + (((size_t)(sfl + pv.max_local - smem) + 15) & ~(size_t)15));
-    float* own_r = own_d + OCAP;
-    float* own_p = own_r + OCAP;
+    const uint32_t OCAP = own_cap<T>(pv.max_own, DPN);
+    T* own_d = reinterpret_cast<T*>(smem + (((size_t)(sfl + pv.max_local - smem) + 15) & ~(size_t)15));
+    T* own_r = own_d + OCAP;
+    T* own_p = own_r + OCAP;
     uint8_t* own_f = reinterpret_cast<uint8_t*>(own_p + OCAP);
     T beta = T(0);
     const T* pold = nullptr;
@@ -325,12 +333,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     };
     // thread 0: D^-1, r, p_old and flags of the patch's own nodes (single buffer, bar[2])
     auto issue_own = [&](int patch) {
+        constexpr int V = 16 / (int)sizeof(T);  // values per 16 bytes
         const int o0 = pv.po[patch], o1 = pv.po[patch + 1];
-        const int a0 = o0 & ~3, n4 = ((o1 + 3) & ~3) - a0;     // values, 16-byte aligned
-        const int f0 = o0 & ~15, nf = ((o1 + 15) & ~15) - f0;  // flags, 16-byte aligned
-        const uint32_t vb = (uint32_t)n4 * 4u;
+        const int a0 = (DPN * o0) & ~(V - 1), nv = ((DPN * o1 + V - 1) & ~(V - 1)) - a0;  // 16-byte aligned
+        const int f0 = o0 & ~15, nf = ((o1 + 15) & ~15) - f0;                             // flags, 16-byte aligned
+        const uint32_t vb = (uint32_t)nv * (uint32_t)sizeof(T);
         mbar_expect_tx(&bar[2], 3u * vb + (uint32_t)nf);
-        if (n4) {
+        if (nv) {
             bulk_g2s(own_d, a.dinv + a0, vb, &bar[2]);
             bulk_g2s(own_r, a.r + a0, vb, &bar[2]);
             bulk_g2s(own_p, pold + a0, vb, &bar[2]);
@@ -403,9 +412,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                 const int u = u0 + g * blockDim.x;
                 if (OWNB && u < nown) {  // from the own-node slices in shared memory
                     fl[g] = own_f[(o0 & 15) + u];
-                    d0[g][0] = own_d[(o0 & 3) + u];
-                    d1[g][0] = own_r[(o0 & 3) + u];
-                    d2[g][0] = own_p[(o0 & 3) + u];
+                    const int base = ((DPN * o0) & (16 / (int)sizeof(T) - 1)) + DPN * u;
+#pragma unroll
+                    for (int c = 0; c < DPN; ++c) {
+                        d0[g][c] = own_d[base + c];
+                        d1[g][c] = own_r[base + c];
+                        d2[g][c] = own_p[base + c];
+                    }
                 } else if (u < nloc) {
                     fl[g] = u < nown ? pv.flags[node[g]] : sffl[u - nown];
 #pragma unroll
