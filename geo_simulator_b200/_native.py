@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(_HERE, "libgeofem.so")
 
 GEO_OK = 0
 GEO_ERR_INVALID_ARG = 1
+GEO_VTK_LEGACY, GEO_VTK_XML, GEO_VTK_XML_NODAL = 0, 1, 2
 GEO_ERR_SINGULAR_JACOBIAN = 2
 GEO_NOT_CONVERGED = 3
 GEO_ERR_BREAKDOWN = 4
@@ -75,6 +76,8 @@ _SIGS = {
     "geo_mesh_download": [_P, _DP, _DP],
     "geo_vtu_render": [_P, _P, _P, _I32, _P, _I32, _DP, _I64, C.POINTER(_I64)],
     "geo_write_vtu": [_P, _P, _P, _I32, _P, _I32, C.c_char_p, C.POINTER(_I64)],
+    "geo_vtk_render": [_P, _P, _I32, _P, _I32, _P, _I32, _DP, _I64, C.POINTER(_I64)],
+    "geo_write_vtk": [_P, _P, _I32, _P, _I32, _P, _I32, C.c_char_p, C.POINTER(_I64)],
     "geo_dofs_create": [_P, _I64, _I32, _DP, _DP, _PP],
     "geo_dofs_num_dirichlet": [_P, C.POINTER(_I64)],
     "geo_dofs_destroy": [_P],

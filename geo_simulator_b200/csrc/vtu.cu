@@ -1,5 +1,6 @@
-// VTU output of a device mesh and its fields: the drop-in for
-// VtkWriter::write_vtu (mesh/vtk_writer.rs:104-265), byte for byte.
+// VTK output of a device mesh and its fields: the drop-in for VtkWriter::write_vtu
+// (mesh/vtk_writer.rs:104-265), VtkWriter::write (legacy .vtk, :13-101) and
+// VtkWriter::write_nodal_vtu (:531-789), byte for byte.
 //
 // The file is ASCII XML in which every coordinate, index and field value is
 // printed with Rust's `{}` (decimal.cuh). The text is produced on the GPU from
@@ -37,15 +38,16 @@ constexpr int kItemsPerBlock = 128;
 constexpr int kStageBytes = 24 * 1024;
 
 // ------------------------------------------------------------------ items
-struct PointsItem {  // "          x y z\n"
+struct PointsItem {  // indent spaces, "x y z\n" (SoA coordinates)
     const double* xyz;
     int64_t n;
+    int indent;
     __device__ int len(int64_t i) const {
-        return 13 + f64_text(xyz[i]).len + f64_text(xyz[n + i]).len + f64_text(xyz[2 * n + i]).len;
+        return indent + 3 + f64_text(xyz[i]).len + f64_text(xyz[n + i]).len + f64_text(xyz[2 * n + i]).len;
     }
     __device__ void write(int64_t i, char* p) const {
-        for (int j = 0; j < 10; ++j) p[j] = ' ';
-        p += 10;
+        for (int j = 0; j < indent; ++j) p[j] = ' ';
+        p += indent;
 #pragma unroll 1
         for (int c = 0; c < 3; ++c) {
             const F64Text t = f64_text(xyz[c * n + i]);
@@ -115,7 +117,78 @@ struct ValuesItem {  // "v " (scalar) or "x y z " (vector): `comps` values per i
     }
 };
 
+struct LineItem {  // indent spaces, then `comps` values separated by ' ', then '\n' (AoS data)
+    const double* v;
+    int comps;
+    int indent;
+    __device__ int len(int64_t i) const {
+        int s = indent + comps;
+        for (int c = 0; c < comps; ++c) s += f64_text(v[comps * i + c]).len;
+        return s;
+    }
+    __device__ void write(int64_t i, char* p) const {
+        for (int j = 0; j < indent; ++j) p[j] = ' ';
+        p += indent;
+#pragma unroll 1
+        for (int c = 0; c < comps; ++c) {
+            const F64Text t = f64_text(v[comps * i + c]);
+            f64_write(t, p);
+            p[t.len] = c + 1 < comps ? ' ' : '\n';
+            p += t.len + 1;
+        }
+    }
+};
+
+struct LegacyCellItem {  // "10 id id ... id\n"
+    const int32_t* conn;
+    int64_t n;
+    __device__ int len(int64_t e) const {
+        int s = 3;
+#pragma unroll
+        for (int j = 0; j < 10; ++j) s += uint_len((uint32_t)conn[j * n + e]) + 1;
+        return s;
+    }
+    __device__ void write(int64_t e, char* p) const {
+        p[0] = '1';
+        p[1] = '0';
+        p += 2;
+#pragma unroll 1
+        for (int j = 0; j < 10; ++j) {
+            const uint32_t v = (uint32_t)conn[j * n + e];
+            const int l = uint_len(v);
+            *p++ = ' ';
+            uint_write(v, l, p);
+            p += l;
+        }
+        *p = '\n';
+    }
+};
+
+struct LegacyTypeItem {  // "24\n"
+    __device__ int len(int64_t) const { return 3; }
+    __device__ void write(int64_t, char* p) const {
+        p[0] = '2';
+        p[1] = '4';
+        p[2] = '\n';
+    }
+};
+
 // ------------------------------------------------------------------ kernels
+// Cell value -> node: the sum over the node's elements in increasing element order
+// (the incidence list is sorted by element), divided by the number of elements when
+// `counted` (write_nodal_vtu averages only when its PlasticStrain pass counted).
+__global__ void k_cell_to_node(const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc,
+                               const double* __restrict__ cell, int64_t N, int counted, double* __restrict__ out) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+        const int b = inc_ptr[n], e = inc_ptr[n + 1];
+        double s = 0.0;
+        if (cell)
+            for (int j = b; j < e; ++j) s += cell[inc[j] / 10];
+        if (counted && e > b) s /= (double)(e - b);
+        out[n] = s;
+    }
+}
+
 template <class Item>
 __global__ void __launch_bounds__(256) k_item_lengths(Item it, int64_t n, int64_t* __restrict__ len,
                                                       unsigned long long* __restrict__ max_len) {
@@ -356,8 +429,8 @@ void emit_fields(Emitter& em, const std::vector<FieldIn>& fields) {
         }
 }
 
-// VtkWriter::write_vtu's sequence of writes (vtk_writer.rs:104-265)
-void emit_vtu(Emitter& em, const geo_mesh* m, const std::vector<FieldIn>& pf, const std::vector<FieldIn>& cf) {
+// The XML header, points and cells shared by write_vtu and write_nodal_vtu (vtk_writer.rs:104-174, :536-576)
+void emit_vtu_head(Emitter& em, const geo_mesh* m) {
     const int64_t N = m->n_nodes, E = m->n_elem;
     em.text("<?xml version=\"1.0\"?>\n"
             "<VTKFile type=\"UnstructuredGrid\" version=\"1.0\" byte_order=\"LittleEndian\">\n"
@@ -366,7 +439,7 @@ void emit_vtu(Emitter& em, const geo_mesh* m, const std::vector<FieldIn>& pf, co
             "\">\n"
             "      <Points>\n"
             "        <DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n");
-    em.section(PointsItem{m->xyz.p, N}, N);
+    em.section(PointsItem{m->xyz.p, N, 10}, N);
     em.text("        </DataArray>\n"
             "      </Points>\n"
             "      <Cells>\n"
@@ -383,6 +456,15 @@ void emit_vtu(Emitter& em, const geo_mesh* m, const std::vector<FieldIn>& pf, co
     em.section(TypesItem{}, E, 3);
     em.text("\n        </DataArray>\n"
             "      </Cells>\n");
+}
+
+const char* const kTail = "    </Piece>\n"
+                          "  </UnstructuredGrid>\n"
+                          "</VTKFile>\n";
+
+// VtkWriter::write_vtu's sequence of writes (vtk_writer.rs:104-265)
+void emit_vtu(Emitter& em, const geo_mesh* m, const std::vector<FieldIn>& pf, const std::vector<FieldIn>& cf) {
+    emit_vtu_head(em, m);
     if (!pf.empty()) {
         em.text("      <PointData>\n");
         emit_fields(em, pf);
@@ -393,10 +475,90 @@ void emit_vtu(Emitter& em, const geo_mesh* m, const std::vector<FieldIn>& pf, co
         emit_fields(em, cf);
         em.text("      </CellData>\n");
     }
-    em.text("    </Piece>\n"
-            "  </UnstructuredGrid>\n"
-            "</VTKFile>\n");
+    em.text(kTail);
     em.finish();
+}
+
+// VtkWriter::write's sequence of writes (vtk_writer.rs:13-101): legacy ASCII .vtk
+void emit_vtk_legacy(Emitter& em, const geo_mesh* m, const std::vector<FieldIn>& pf,
+                     const std::vector<FieldIn>& cf) {
+    const int64_t N = m->n_nodes, E = m->n_elem;
+    em.text("# vtk DataFile Version 3.0\n"
+            "Tet10 Mesh generated by geo_simulator\n"
+            "ASCII\n"
+            "DATASET UNSTRUCTURED_GRID\n"
+            "POINTS " + std::to_string(N) + " double\n");
+    em.section(PointsItem{m->xyz.p, N, 0}, N);
+    em.text("\nCELLS " + std::to_string(E) + " " + std::to_string(11 * E) + "\n");
+    em.section(LegacyCellItem{m->conn.p, E}, E);
+    em.text("\nCELL_TYPES " + std::to_string(E) + "\n");
+    em.section(LegacyTypeItem{}, E, 3);
+    auto block = [&](const char* tag, int64_t count, const std::vector<FieldIn>& fields) {
+        if (fields.empty()) return;
+        em.text(std::string("\n") + tag + " " + std::to_string(count) + "\n");
+        for (int pass = 0; pass < 2; ++pass)
+            for (const FieldIn& f : fields) {
+                const bool vec = f.comps == 3;
+                if (vec != (pass == 1)) continue;
+                em.text(vec ? "VECTORS " + f.name + " double\n"
+                            : "SCALARS " + f.name + " double 1\nLOOKUP_TABLE default\n");
+                em.section(LineItem{em.stage(f.data, (size_t)(f.count * f.comps)), f.comps, 0}, f.count);
+            }
+    };
+    block("POINT_DATA", N, pf);
+    block("CELL_DATA", E, cf);
+    em.finish();
+}
+
+// the nine cell fields write_nodal_vtu averages to the nodes, in its output order
+const char* const kNodalNames[9] = {"PlasticStrain", "Stress_II",   "StrainRate_II",    "Pressure",        "Viscosity",
+                                    "IsYielding",    "YieldStress", "PlasticViscosity", "SoftenedCohesion"};
+
+// VtkWriter::write_nodal_vtu's sequence of writes (vtk_writer.rs:531-789)
+void emit_vtu_nodal(Emitter& em, geo_mesh* m, const std::vector<FieldIn>& pf, const std::vector<FieldIn>& cf) {
+    const int64_t N = m->n_nodes;
+    const FieldIn* src[9] = {};
+    for (int k = 0; k < 9; ++k)
+        for (const FieldIn& f : cf)
+            if (f.comps == 1 && f.name == kNodalNames[k]) src[k] = &f;  // the map keeps the last of a name
+    for (const FieldIn* f : src)
+        if (f) GEO_CHECK_ARG(f->count >= m->n_elem, "nodal VTU: a named cell field has fewer values than cells");
+    emit_vtu_head(em, m);
+    em.text("      <PointData>\n");
+    for (const FieldIn& f : pf) {
+        if (f.comps != 3) continue;
+        em.text("        <DataArray type=\"Float64\" Name=\"" + f.name +
+                "\" NumberOfComponents=\"3\" format=\"ascii\">\n");
+        em.section(LineItem{em.stage(f.data, (size_t)(f.count * 3)), 3, 10}, f.count);
+        em.text("        </DataArray>\n");
+    }
+    auto scalar = [&](const std::string& name, const double* v, int64_t n) {
+        em.text("        <DataArray type=\"Float64\" Name=\"" + name + "\" format=\"ascii\">\n          ");
+        em.section(ValuesItem{v, 1}, n);
+        em.text("\n        </DataArray>\n");
+    };
+    for (const FieldIn& f : pf)
+        if (f.comps == 1) scalar(f.name, em.stage(f.data, (size_t)f.count), f.count);
+    ensure_inverse_map(m);
+    geo_ctx* ctx = m->ctx;
+    for (int k = 0; k < 9; ++k) {
+        const double* cell = src[k] ? em.stage(src[k]->data, (size_t)m->n_elem) : nullptr;
+        double* nodal = ctx_scratch<double>(ctx, SCR_IN2, (size_t)N);
+        k_cell_to_node<<<(unsigned)std::min<int64_t>(cdiv(N, 256), (int64_t)ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+            m->inc_ptr.p, m->inc.p, cell, N, src[0] != nullptr, nodal);
+        check_launch(ctx, "k_cell_to_node");
+        scalar(kNodalNames[k], nodal, N);
+    }
+    em.text("      </PointData>\n");
+    em.text(kTail);
+    em.finish();
+}
+
+void emit_format(Emitter& em, geo_mesh* m, int format, const std::vector<FieldIn>& pf,
+                 const std::vector<FieldIn>& cf) {
+    if (format == GEO_VTK_LEGACY) emit_vtk_legacy(em, m, pf, cf);
+    else if (format == GEO_VTK_XML_NODAL) emit_vtu_nodal(em, m, pf, cf);
+    else emit_vtu(em, m, pf, cf);
 }
 
 std::vector<FieldIn> check_fields(const geo_vtu_field* f, int32_t n) {
@@ -418,30 +580,35 @@ using namespace geo;
 
 extern "C" {
 
-int geo_vtu_render(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point_fields, int32_t n_point,
-                   const geo_vtu_field* cell_fields, int32_t n_cell, char* out, int64_t capacity, int64_t* size) {
+int geo_vtk_render(geo_ctx* ctx, const geo_mesh* mesh, int32_t format, const geo_vtu_field* point_fields,
+                   int32_t n_point, const geo_vtu_field* cell_fields, int32_t n_cell, char* out, int64_t capacity,
+                   int64_t* size) {
     GEO_API_BEGIN(ctx)
     GEO_CHECK_ARG(ctx && mesh && size, "ctx/mesh/size is NULL");
+    GEO_CHECK_ARG(format == GEO_VTK_LEGACY || format == GEO_VTK_XML || format == GEO_VTK_XML_NODAL,
+                  "unknown VTK format");
     const auto pf = check_fields(point_fields, n_point);
     const auto cf = check_fields(cell_fields, n_cell);
     Emitter em(ctx, out ? (is_device_ptr(out) ? TO_DEVICE : TO_HOST) : SIZE_ONLY, out, out ? capacity : 0, nullptr);
-    emit_vtu(em, mesh, pf, cf);
+    emit_format(em, const_cast<geo_mesh*>(mesh), format, pf, cf);
     *size = em.pos();
     if (em.overflow()) fail(GEO_ERR_INVALID_ARG, "output buffer too small (size holds the required bytes)");
     GEO_API_END
 }
 
-int geo_write_vtu(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point_fields, int32_t n_point,
-                  const geo_vtu_field* cell_fields, int32_t n_cell, const char* path, int64_t* size) {
+int geo_write_vtk(geo_ctx* ctx, const geo_mesh* mesh, int32_t format, const geo_vtu_field* point_fields,
+                  int32_t n_point, const geo_vtu_field* cell_fields, int32_t n_cell, const char* path, int64_t* size) {
     GEO_API_BEGIN(ctx)
     GEO_CHECK_ARG(ctx && mesh && path, "ctx/mesh/path is NULL");
+    GEO_CHECK_ARG(format == GEO_VTK_LEGACY || format == GEO_VTK_XML || format == GEO_VTK_XML_NODAL,
+                  "unknown VTK format");
     const auto pf = check_fields(point_fields, n_point);
     const auto cf = check_fields(cell_fields, n_cell);
     FILE* fp = std::fopen(path, "wb");
     if (!fp) fail(GEO_ERR_INVALID_ARG, std::string("cannot create ") + path);
     try {
         Emitter em(ctx, TO_FILE, nullptr, 0, fp);
-        emit_vtu(em, mesh, pf, cf);
+        emit_format(em, const_cast<geo_mesh*>(mesh), format, pf, cf);
         if (size) *size = em.pos();
     } catch (...) {
         std::fclose(fp);
@@ -449,6 +616,16 @@ int geo_write_vtu(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point
     }
     if (std::fclose(fp) != 0) fail(GEO_ERR_INVALID_ARG, "closing the output file failed");
     GEO_API_END
+}
+
+int geo_vtu_render(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point_fields, int32_t n_point,
+                   const geo_vtu_field* cell_fields, int32_t n_cell, char* out, int64_t capacity, int64_t* size) {
+    return geo_vtk_render(ctx, mesh, GEO_VTK_XML, point_fields, n_point, cell_fields, n_cell, out, capacity, size);
+}
+
+int geo_write_vtu(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point_fields, int32_t n_point,
+                  const geo_vtu_field* cell_fields, int32_t n_cell, const char* path, int64_t* size) {
+    return geo_write_vtk(ctx, mesh, GEO_VTK_XML, point_fields, n_point, cell_fields, n_cell, path, size);
 }
 
 }  // extern "C"

@@ -312,37 +312,116 @@ def _vtu_fields(fd: FieldData):
 
 
 class VtkWriter:
-    """mesh/vtk_writer.rs:7-265: ``write_vtu`` renders the text on the GPU, byte for
-    byte as the reference (Rust ``{}`` for every number)."""
+    """mesh/vtk_writer.rs:7-789: the text is rendered on the GPU, byte for byte as
+    the reference's writers (Rust ``{}`` for every number)."""
 
     @staticmethod
-    def write_vtu(mesh: Mesh, filename: str, ctx=None) -> int:
-        """VtkWriter::write_vtu (vtk_writer.rs:104-265); returns the bytes written."""
-        ctx = _ctx(ctx)
-        pf, npf, k1 = _vtu_fields(mesh.field_data)
-        cf, ncf, k2 = _vtu_fields(mesh.cell_data)
-        size = C.c_int64()
-        ctx.check(N.lib().geo_write_vtu(ctx.h, mesh.handle(ctx), pf, npf, cf, ncf, str(filename).encode(),
-                                        C.byref(size)))
-        return int(size.value)
-
-    @staticmethod
-    def render_vtu(mesh: Mesh, out=None, ctx=None):
-        """The same text as bytes (out None), or into ``out`` (a uint8 numpy array or
-        CUDA tensor large enough); returns the bytes or the size."""
+    def _out(mesh, fmt, filename, out, ctx):
         ctx = _ctx(ctx)
         pf, npf, k1 = _vtu_fields(mesh.field_data)
         cf, ncf, k2 = _vtu_fields(mesh.cell_data)
         L = N.lib()
         size = C.c_int64()
+        h = mesh.handle(ctx)
+        if filename is not None:
+            ctx.check(L.geo_write_vtk(ctx.h, h, fmt, pf, npf, cf, ncf, str(filename).encode(), C.byref(size)))
+            return int(size.value)
         if out is not None:
             cap = out.numel() if hasattr(out, "numel") else out.size
-            ctx.check(L.geo_vtu_render(ctx.h, mesh.handle(ctx), pf, npf, cf, ncf, _ptr(out), cap, C.byref(size)))
+            ctx.check(L.geo_vtk_render(ctx.h, h, fmt, pf, npf, cf, ncf, _ptr(out), cap, C.byref(size)))
             return int(size.value)
-        ctx.check(L.geo_vtu_render(ctx.h, mesh.handle(ctx), pf, npf, cf, ncf, None, 0, C.byref(size)))
+        ctx.check(L.geo_vtk_render(ctx.h, h, fmt, pf, npf, cf, ncf, None, 0, C.byref(size)))
         buf = np.empty(int(size.value), np.uint8)
-        ctx.check(L.geo_vtu_render(ctx.h, mesh.handle(ctx), pf, npf, cf, ncf, _ptr(buf), buf.size, C.byref(size)))
+        ctx.check(L.geo_vtk_render(ctx.h, h, fmt, pf, npf, cf, ncf, _ptr(buf), buf.size, C.byref(size)))
         return buf.tobytes()
+
+    @staticmethod
+    def write(mesh: Mesh, filename: str, ctx=None) -> int:
+        """VtkWriter::write (vtk_writer.rs:13-101): legacy ASCII .vtk; returns the bytes written."""
+        return VtkWriter._out(mesh, N.GEO_VTK_LEGACY, filename, None, ctx)
+
+    @staticmethod
+    def write_vtu(mesh: Mesh, filename: str, ctx=None) -> int:
+        """VtkWriter::write_vtu (vtk_writer.rs:104-265); returns the bytes written."""
+        return VtkWriter._out(mesh, N.GEO_VTK_XML, filename, None, ctx)
+
+    @staticmethod
+    def write_nodal_vtu(mesh: Mesh, tracers, filename: str, ctx=None) -> int:
+        """VtkWriter::write_nodal_vtu (vtk_writer.rs:531-789); the tracers are unused, as
+        in the reference. Returns the bytes written."""
+        return VtkWriter._out(mesh, N.GEO_VTK_XML_NODAL, filename, None, ctx)
+
+    @staticmethod
+    def render_vtu(mesh: Mesh, out=None, ctx=None, fmt=None):
+        """The text of write_vtu (or of ``fmt``: GEO_VTK_LEGACY / _XML / _XML_NODAL) as
+        bytes (out None), or into ``out`` (a uint8 numpy array or CUDA tensor large
+        enough); returns the bytes or the size."""
+        return VtkWriter._out(mesh, N.GEO_VTK_XML if fmt is None else fmt, None, out, ctx)
+
+
+class VtkFormat:
+    """vtk_writer.rs:791-845."""
+    Legacy, Xml, XmlNodal, XmlMultiBlock = "Legacy", "Xml", "XmlNodal", "XmlMultiBlock"
+    _EXT = {"Legacy": ".vtk", "Xml": ".vtu", "XmlNodal": ".vtu", "XmlMultiBlock": ".vtm"}
+
+    @staticmethod
+    def extension(fmt) -> str:
+        return VtkFormat._EXT[fmt]
+
+    @staticmethod
+    def from_filename(filename: str):
+        if filename.endswith(".vtk"):
+            return VtkFormat.Legacy
+        if filename.endswith(".vtu"):
+            return VtkFormat.XmlNodal  # the reference's default for .vtu
+        if filename.endswith(".vtm"):
+            return VtkFormat.XmlMultiBlock
+        return None
+
+
+class VtkOutputBuilder:
+    """vtk_writer.rs:847-985 (default format XmlNodal; with_fields is stored but, as in
+    the reference, not applied). The tracer multi-block format has no GPU writer here."""
+
+    def __init__(self, mesh: Mesh):
+        self.mesh, self.tracers, self.format, self.fields = mesh, None, VtkFormat.XmlNodal, None
+
+    new = classmethod(lambda cls, mesh: cls(mesh))
+
+    def with_tracers(self, tracers):
+        self.tracers = tracers
+        return self
+
+    def with_format(self, fmt):
+        self.format = fmt
+        return self
+
+    def with_fields(self, fields):
+        self.fields = list(fields)
+        return self
+
+    def auto_format(self, filename: str):
+        fmt = VtkFormat.from_filename(filename)
+        if fmt is not None:
+            self.format = fmt
+        return self
+
+    def write(self, filename: str, ctx=None) -> int:
+        if self.format == VtkFormat.Legacy:
+            return VtkWriter.write(self.mesh, filename, ctx)
+        if self.format == VtkFormat.Xml:
+            return VtkWriter.write_vtu(self.mesh, filename, ctx)
+        if self.format == VtkFormat.XmlNodal:
+            return VtkWriter.write_nodal_vtu(self.mesh, self.tracers, filename, ctx)
+        raise GeoError(N.GEO_ERR_UNSUPPORTED, "the multi-block tracer format (write_combined_vtu) is not supported")
+
+    def recommended_filename(self, base: str) -> str:
+        return base + VtkFormat.extension(self.format)
+
+
+def quick_write_vtu(mesh: Mesh, filename: str, ctx=None) -> int:
+    """vtk_writer.rs:986-988: the builder's default (nodal) format."""
+    return VtkOutputBuilder(mesh).write(filename, ctx)
 
 
 # --------------------------------------------------------------------------- DOFs

@@ -149,6 +149,25 @@ int geo_vtu_render(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* poin
 int geo_write_vtu(geo_ctx* ctx, const geo_mesh* mesh, const geo_vtu_field* point_fields, int32_t n_point,
                   const geo_vtu_field* cell_fields, int32_t n_cell, const char* path, int64_t* size);
 
+/* The reference's other writers with the same fields and sinks, selected by format:
+ * GEO_VTK_LEGACY    VtkWriter::write, mesh/vtk_writer.rs:13-101 (legacy ASCII .vtk);
+ * GEO_VTK_XML       VtkWriter::write_vtu (as geo_vtu_render / geo_write_vtu);
+ * GEO_VTK_XML_NODAL VtkWriter::write_nodal_vtu, :531-789 (the builder's default):
+ *                   vector point fields one per line, scalar point fields, then
+ *                   the named cell fields PlasticStrain, Stress_II, StrainRate_II,
+ *                   Pressure, Viscosity, IsYielding, YieldStress, PlasticViscosity
+ *                   and SoftenedCohesion summed to the nodes in element order,
+ *                   divided by the node's element count only when PlasticStrain
+ *                   is present, zero when absent; no CellData.              */
+#define GEO_VTK_LEGACY 0
+#define GEO_VTK_XML 1
+#define GEO_VTK_XML_NODAL 2
+int geo_vtk_render(geo_ctx* ctx, const geo_mesh* mesh, int32_t format, const geo_vtu_field* point_fields,
+                   int32_t n_point, const geo_vtu_field* cell_fields, int32_t n_cell, char* out, int64_t capacity,
+                   int64_t* size);
+int geo_write_vtk(geo_ctx* ctx, const geo_mesh* mesh, int32_t format, const geo_vtu_field* point_fields,
+                  int32_t n_point, const geo_vtu_field* cell_fields, int32_t n_cell, const char* path, int64_t* size);
+
 /* DofManager::new + set_dirichlet, dof.rs:37-50, :113-130. dirichlet_mask[n_dofs]
  * (nonzero = constrained) and dirichlet_values[n_dofs]; either may be NULL.     */
 int geo_dofs_create(geo_ctx* ctx, int64_t n_nodes, int32_t dofs_per_node,

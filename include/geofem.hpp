@@ -17,7 +17,8 @@
 //   SolverStats (src/linalg/solver.rs:5-32)            geofem::SolverStats
 //   CsMat<f64> (sprs)                                  geofem::CsMat (device-resident CSR)
 //   FieldData / ScalarField / VectorField (mesh/fields.rs) geofem::FieldData / ScalarField / VectorField
-//   VtkWriter::write_vtu (mesh/vtk_writer.rs:104-265)  geofem::VtkWriter::write_vtu / render_vtu (GPU text)
+//   VtkWriter::write / write_vtu / write_nodal_vtu     geofem::VtkWriter::write / write_vtu / write_nodal_vtu
+//     (mesh/vtk_writer.rs:13-789)                        / render (GPU text)
 //
 // plus the matrix-free operators, the mixed-precision solve and the adjoint
 // (geofem::ThermalOperator / ElasticityOperator with forward and vjp), which
@@ -203,28 +204,45 @@ struct ImprovedMeshGenerator {
     }
 };
 
-// mesh/vtk_writer.rs:104-265: the VTU text rendered on the GPU, byte for byte.
+// mesh/vtk_writer.rs:13-789: the VTK writers, with the text rendered on the GPU byte for byte.
 struct VtkWriter {
+    // VtkWriter::write (vtk_writer.rs:13-101): legacy ASCII .vtk
+    static size_t write(const Mesh& mesh, const std::string& filename, Context& ctx = Context::default_context()) {
+        return to_file(mesh, GEO_VTK_LEGACY, filename, ctx);
+    }
+    // VtkWriter::write_vtu (vtk_writer.rs:104-265)
     static size_t write_vtu(const Mesh& mesh, const std::string& filename,
                             Context& ctx = Context::default_context()) {
+        return to_file(mesh, GEO_VTK_XML, filename, ctx);
+    }
+    // VtkWriter::write_nodal_vtu (vtk_writer.rs:531-789); the reference ignores its tracers
+    static size_t write_nodal_vtu(const Mesh& mesh, const std::string& filename,
+                                  Context& ctx = Context::default_context()) {
+        return to_file(mesh, GEO_VTK_XML_NODAL, filename, ctx);
+    }
+    // the text of one of the writers (GEO_VTK_LEGACY / GEO_VTK_XML / GEO_VTK_XML_NODAL) in memory
+    static std::string render(const Mesh& mesh, int format = GEO_VTK_XML, Context& ctx = Context::default_context()) {
         Fields f(mesh);
         int64_t size = 0;
-        ctx.check(geo_write_vtu(ctx.get(), mesh.handle(ctx), f.point.data(), (int32_t)f.point.size(), f.cell.data(),
-                                (int32_t)f.cell.size(), filename.c_str(), &size));
-        return (size_t)size;
+        ctx.check(geo_vtk_render(ctx.get(), mesh.handle(ctx), format, f.point.data(), (int32_t)f.point.size(),
+                                 f.cell.data(), (int32_t)f.cell.size(), nullptr, 0, &size));
+        std::string out((size_t)size, '\0');
+        ctx.check(geo_vtk_render(ctx.get(), mesh.handle(ctx), format, f.point.data(), (int32_t)f.point.size(),
+                                 f.cell.data(), (int32_t)f.cell.size(), &out[0], size, &size));
+        return out;
     }
     static std::string render_vtu(const Mesh& mesh, Context& ctx = Context::default_context()) {
-        Fields f(mesh);
-        int64_t size = 0;
-        ctx.check(geo_vtu_render(ctx.get(), mesh.handle(ctx), f.point.data(), (int32_t)f.point.size(), f.cell.data(),
-                                 (int32_t)f.cell.size(), nullptr, 0, &size));
-        std::string out((size_t)size, '\0');
-        ctx.check(geo_vtu_render(ctx.get(), mesh.handle(ctx), f.point.data(), (int32_t)f.point.size(), f.cell.data(),
-                                 (int32_t)f.cell.size(), &out[0], size, &size));
-        return out;
+        return render(mesh, GEO_VTK_XML, ctx);
     }
 
 private:
+    static size_t to_file(const Mesh& mesh, int format, const std::string& filename, Context& ctx) {
+        Fields f(mesh);
+        int64_t size = 0;
+        ctx.check(geo_write_vtk(ctx.get(), mesh.handle(ctx), format, f.point.data(), (int32_t)f.point.size(),
+                                f.cell.data(), (int32_t)f.cell.size(), filename.c_str(), &size));
+        return (size_t)size;
+    }
     struct Fields {
         std::vector<geo_vtu_field> point, cell;
         explicit Fields(const Mesh& m) {

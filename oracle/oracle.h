@@ -134,6 +134,17 @@ int64_t orc_write_vtu(int64_t n_nodes, const double* xyz, int64_t n_elem, const 
                       const int32_t* p_comps, int n_cell, const char* const* c_names, const double* const* c_data,
                       const int64_t* c_counts, const int32_t* c_comps, char* out, int64_t cap);
 
+/* VtkWriter::write (vtk_writer.rs:13-101) and write_nodal_vtu (:531-789); same arguments as orc_write_vtu. */
+int64_t orc_write_vtk(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn, int n_point,
+                      const char* const* p_names, const double* const* p_data, const int64_t* p_counts,
+                      const int32_t* p_comps, int n_cell, const char* const* c_names, const double* const* c_data,
+                      const int64_t* c_counts, const int32_t* c_comps, char* out, int64_t cap);
+int64_t orc_write_vtu_nodal(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn, int n_point,
+                            const char* const* p_names, const double* const* p_data, const int64_t* p_counts,
+                            const int32_t* p_comps, int n_cell, const char* const* c_names,
+                            const double* const* c_data, const int64_t* c_counts, const int32_t* c_comps, char* out,
+                            int64_t cap);
+
 #ifdef __cplusplus
 }
 #endif

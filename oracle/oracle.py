@@ -107,6 +107,12 @@ def _declare(L):
         "orc_write_vtu": (C.c_int64, [C.c_int64, _D, C.c_int64, _I64, C.c_int, C.c_void_p, C.c_void_p, _I64,
                                       C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _I64, C.c_void_p,
                                       C.c_char_p, C.c_int64]),
+        "orc_write_vtk": (C.c_int64, [C.c_int64, _D, C.c_int64, _I64, C.c_int, C.c_void_p, C.c_void_p, _I64,
+                                      C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _I64, C.c_void_p,
+                                      C.c_char_p, C.c_int64]),
+        "orc_write_vtu_nodal": (C.c_int64, [C.c_int64, _D, C.c_int64, _I64, C.c_int, C.c_void_p, C.c_void_p,
+                                            _I64, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _I64, C.c_void_p,
+                                            C.c_char_p, C.c_int64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -523,9 +529,11 @@ def _field_arrays(fields):
     return n, names, ptrs, counts, comps, arrs
 
 
-def write_vtu(xyz, conn, point_fields=(), cell_fields=()) -> bytes:
-    """VtkWriter::write_vtu (mesh/vtk_writer.rs:104-265) as bytes. Fields are
+def write_vtu(xyz, conn, point_fields=(), cell_fields=(), fmt="xml") -> bytes:
+    """VtkWriter::write_vtu (mesh/vtk_writer.rs:104-265) as bytes; fmt "legacy" gives
+    VtkWriter::write (:13-101), "nodal" write_nodal_vtu (:531-789). Fields are
     (name, data, components) with components 1 (scalar) or 3 (vector, [n][3])."""
+    fn = {"xml": "orc_write_vtu", "legacy": "orc_write_vtk", "nodal": "orc_write_vtu_nodal"}[fmt]
     xyz = _f64(xyz)
     conn = _i64(conn)
     np_, pn, pp, pc, pk, keep_p = _field_arrays(list(point_fields))
@@ -533,7 +541,8 @@ def write_vtu(xyz, conn, point_fields=(), cell_fields=()) -> bytes:
     L = lib()
     args = (xyz.shape[0], _d(xyz), conn.shape[0], _i(conn), np_, pn, pp, _i(pc), pk.ctypes.data, nc, cn, cp,
             _i(cc), ck.ctypes.data)
-    size = L.orc_write_vtu(*args, None, 0)
+    f = getattr(L, fn)
+    size = f(*args, None, 0)
     out = C.create_string_buffer(int(size))
-    L.orc_write_vtu(*args, out, size)
+    f(*args, out, size)
     return out.raw[:size]

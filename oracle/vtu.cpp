@@ -183,9 +183,182 @@ void put_fields(std::string& out, int n_fields, const char* const* names, const 
         }
 }
 
+const char* const kNodalNames[9] = {"PlasticStrain",    "Stress_II",   "StrainRate_II",
+                                     "Pressure",         "Viscosity",   "IsYielding",
+                                     "YieldStress",      "PlasticViscosity", "SoftenedCohesion"};
+
 }  // namespace
 
 extern "C" {
+
+// VtkWriter::write (mesh/vtk_writer.rs:13-101): legacy ASCII .vtk
+int64_t orc_write_vtk(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn, int n_point,
+                      const char* const* p_names, const double* const* p_data, const int64_t* p_counts,
+                      const int32_t* p_comps, int n_cell, const char* const* c_names, const double* const* c_data,
+                      const int64_t* c_counts, const int32_t* c_comps, char* out, int64_t cap) {
+    std::string s;
+    s += "# vtk DataFile Version 3.0\n";
+    s += "Tet10 Mesh generated by geo_simulator\n";
+    s += "ASCII\n";
+    s += "DATASET UNSTRUCTURED_GRID\n";
+    s += "POINTS " + std::to_string(n_nodes) + " double\n";
+    for (int64_t i = 0; i < n_nodes; ++i) {
+        put_f64(s, xyz[3 * i]);
+        s.push_back(' ');
+        put_f64(s, xyz[3 * i + 1]);
+        s.push_back(' ');
+        put_f64(s, xyz[3 * i + 2]);
+        s.push_back('\n');
+    }
+    s += "\nCELLS " + std::to_string(n_elem) + " " + std::to_string(11 * n_elem) + "\n";
+    for (int64_t e = 0; e < n_elem; ++e) {
+        s += "10";
+        for (int l = 0; l < 10; ++l) {
+            s.push_back(' ');
+            put_int(s, conn[10 * e + l]);
+        }
+        s.push_back('\n');
+    }
+    s += "\nCELL_TYPES " + std::to_string(n_elem) + "\n";
+    for (int64_t e = 0; e < n_elem; ++e) s += "24\n";
+    auto block = [&](const char* tag, int64_t count, int nf, const char* const* names, const double* const* data,
+                     const int64_t* counts, const int32_t* comps) {
+        if (nf <= 0) return;
+        s += std::string("\n") + tag + " " + std::to_string(count) + "\n";
+        for (int pass = 0; pass < 2; ++pass)
+            for (int f = 0; f < nf; ++f) {
+                const bool vec = comps[f] == 3;
+                if (vec != (pass == 1)) continue;
+                if (!vec) {
+                    s += std::string("SCALARS ") + names[f] + " double 1\n";
+                    s += "LOOKUP_TABLE default\n";
+                    for (int64_t i = 0; i < counts[f]; ++i) {
+                        put_f64(s, data[f][i]);
+                        s.push_back('\n');
+                    }
+                } else {
+                    s += std::string("VECTORS ") + names[f] + " double\n";
+                    for (int64_t i = 0; i < counts[f]; ++i) {
+                        put_f64(s, data[f][3 * i]);
+                        s.push_back(' ');
+                        put_f64(s, data[f][3 * i + 1]);
+                        s.push_back(' ');
+                        put_f64(s, data[f][3 * i + 2]);
+                        s.push_back('\n');
+                    }
+                }
+            }
+    };
+    block("POINT_DATA", n_nodes, n_point, p_names, p_data, p_counts, p_comps);
+    block("CELL_DATA", n_elem, n_cell, c_names, c_data, c_counts, c_comps);
+    if (out && (int64_t)s.size() <= cap) std::memcpy(out, s.data(), s.size());
+    return (int64_t)s.size();
+}
+
+// VtkWriter::write_nodal_vtu (mesh/vtk_writer.rs:531-789): points and cells as in
+// write_vtu; PointData holds the vector point fields (one vector per line), the
+// scalar point fields, then nine named cell fields averaged to the nodes (summed
+// per node in element order; divided by the count that only the PlasticStrain
+// pass increments; a missing field leaves zeros). No CellData. Cell fields must
+// hold at least n_elem values.
+int64_t orc_write_vtu_nodal(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn, int n_point,
+                            const char* const* p_names, const double* const* p_data, const int64_t* p_counts,
+                            const int32_t* p_comps, int n_cell, const char* const* c_names,
+                            const double* const* c_data, const int64_t* c_counts, const int32_t* c_comps, char* out,
+                            int64_t cap) {
+    std::string s;
+    s += "<?xml version=\"1.0\"?>\n";
+    s += "<VTKFile type=\"UnstructuredGrid\" version=\"1.0\" byte_order=\"LittleEndian\">\n";
+    s += "  <UnstructuredGrid>\n";
+    s += "    <Piece NumberOfPoints=\"" + std::to_string(n_nodes) + "\" NumberOfCells=\"" + std::to_string(n_elem) +
+         "\">\n";
+    s += "      <Points>\n";
+    s += "        <DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n";
+    for (int64_t i = 0; i < n_nodes; ++i) {
+        s += "          ";
+        put_f64(s, xyz[3 * i]);
+        s.push_back(' ');
+        put_f64(s, xyz[3 * i + 1]);
+        s.push_back(' ');
+        put_f64(s, xyz[3 * i + 2]);
+        s.push_back('\n');
+    }
+    s += "        </DataArray>\n";
+    s += "      </Points>\n";
+    s += "      <Cells>\n";
+    s += "        <DataArray type=\"Int32\" Name=\"connectivity\" format=\"ascii\">\n";
+    s += "          ";
+    for (int64_t i = 0; i < 10 * n_elem; ++i) {
+        put_int(s, conn[i]);
+        s.push_back(' ');
+    }
+    s += "\n        </DataArray>\n";
+    s += "        <DataArray type=\"Int32\" Name=\"offsets\" format=\"ascii\">\n";
+    s += "          ";
+    for (int64_t i = 1; i <= n_elem; ++i) {
+        put_int(s, 10 * i);
+        s.push_back(' ');
+    }
+    s += "\n        </DataArray>\n";
+    s += "        <DataArray type=\"UInt8\" Name=\"types\" format=\"ascii\">\n";
+    s += "          ";
+    for (int64_t i = 0; i < n_elem; ++i) s += "24 ";
+    s += "\n        </DataArray>\n";
+    s += "      </Cells>\n";
+    // cell -> node averaging of the nine named fields
+    std::vector<std::vector<double>> nodal(9, std::vector<double>((size_t)n_nodes, 0.0));
+    std::vector<int64_t> count((size_t)n_nodes, 0);
+    for (int k = 0; k < 9; ++k) {
+        const double* src = nullptr;
+        for (int f = 0; f < n_cell; ++f)
+            if (c_comps[f] == 1 && std::strcmp(c_names[f], kNodalNames[k]) == 0) src = c_data[f];
+        if (!src) continue;
+        for (int64_t e = 0; e < n_elem; ++e)
+            for (int l = 0; l < 10; ++l) {
+                const int64_t n = conn[10 * e + l];
+                nodal[k][(size_t)n] += src[e];
+                if (k == 0) ++count[(size_t)n];
+            }
+    }
+    for (int64_t i = 0; i < n_nodes; ++i)
+        if (count[(size_t)i] > 0)
+            for (int k = 0; k < 9; ++k) nodal[k][(size_t)i] /= (double)count[(size_t)i];
+    s += "      <PointData>\n";
+    for (int f = 0; f < n_point; ++f) {
+        if (p_comps[f] != 3) continue;
+        s += std::string("        <DataArray type=\"Float64\" Name=\"") + p_names[f] +
+             "\" NumberOfComponents=\"3\" format=\"ascii\">\n";
+        for (int64_t i = 0; i < p_counts[f]; ++i) {
+            s += "          ";
+            put_f64(s, p_data[f][3 * i]);
+            s.push_back(' ');
+            put_f64(s, p_data[f][3 * i + 1]);
+            s.push_back(' ');
+            put_f64(s, p_data[f][3 * i + 2]);
+            s.push_back('\n');
+        }
+        s += "        </DataArray>\n";
+    }
+    auto scalar_array = [&](const char* name, const double* v, int64_t n) {
+        s += std::string("        <DataArray type=\"Float64\" Name=\"") + name + "\" format=\"ascii\">\n";
+        s += "          ";
+        for (int64_t i = 0; i < n; ++i) {
+            put_f64(s, v[i]);
+            s.push_back(' ');
+        }
+        s += "\n        </DataArray>\n";
+    };
+    for (int f = 0; f < n_point; ++f)
+        if (p_comps[f] == 1) scalar_array(p_names[f], p_data[f], p_counts[f]);
+    for (int k = 0; k < 9; ++k) scalar_array(kNodalNames[k], nodal[k].data(), n_nodes);
+    s += "      </PointData>\n";
+    s += "    </Piece>\n";
+    s += "  </UnstructuredGrid>\n";
+    s += "</VTKFile>\n";
+    (void)c_counts;
+    if (out && (int64_t)s.size() <= cap) std::memcpy(out, s.data(), s.size());
+    return (int64_t)s.size();
+}
 
 int orc_format_f64(double v, char* out, int cap) {
     std::string s;

@@ -330,6 +330,15 @@ void vtu_output() {
     }
     std::remove(path);
     expect(n == text.size() && back == text, "write_vtu streams the same bytes as render_vtu");
+    const std::string legacy = VtkWriter::render(mesh, GEO_VTK_LEGACY);
+    expect(legacy.rfind("# vtk DataFile Version 3.0\nTet10 Mesh generated by geo_simulator\nASCII\n", 0) == 0 &&
+               legacy.find("\nCELLS 12 132\n10 ") != std::string::npos &&
+               legacy.find("SCALARS T double 1\nLOOKUP_TABLE default\n0.30000000000000004\n-0\n") != std::string::npos,
+           "legacy VTK layout as VtkWriter::write");
+    const std::string nodal = VtkWriter::render(mesh, GEO_VTK_XML_NODAL);
+    expect(nodal.find("Name=\"SoftenedCohesion\" format=\"ascii\">\n          0 0 ") != std::string::npos &&
+               nodal.find("<CellData>") == std::string::npos,
+           "nodal VTU: the named plasticity fields default to zero, no CellData");
 }
 
 }  // namespace

@@ -99,6 +99,80 @@ def python_write_vtu(xyz, conn, pf, cf) -> bytes:
     return "".join(out).encode()
 
 
+NODAL_NAMES = ["PlasticStrain", "Stress_II", "StrainRate_II", "Pressure", "Viscosity", "IsYielding",
+               "YieldStress", "PlasticViscosity", "SoftenedCohesion"]
+
+
+def python_write_vtk(xyz, conn, pf, cf) -> bytes:
+    """A second restatement of VtkWriter::write (vtk_writer.rs:13-101)."""
+    f = rust_display_from_repr
+    out = ["# vtk DataFile Version 3.0\n", "Tet10 Mesh generated by geo_simulator\n", "ASCII\n",
+           "DATASET UNSTRUCTURED_GRID\n", f"POINTS {xyz.shape[0]} double\n"]
+    out += [f"{f(p[0])} {f(p[1])} {f(p[2])}\n" for p in xyz]
+    out.append(f"\nCELLS {conn.shape[0]} {11 * conn.shape[0]}\n")
+    out += ["10" + "".join(f" {int(i)}" for i in row) + "\n" for row in conn]
+    out.append(f"\nCELL_TYPES {conn.shape[0]}\n")
+    out += ["24\n"] * conn.shape[0]
+    for tag, count, fields in (("POINT_DATA", xyz.shape[0], pf), ("CELL_DATA", conn.shape[0], cf)):
+        if not fields:
+            continue
+        out.append(f"\n{tag} {count}\n")
+        for vec in (False, True):
+            for name, data, comps in fields:
+                if (comps == 3) != vec:
+                    continue
+                d = np.asarray(data, np.float64).reshape(-1, comps)
+                if vec:
+                    out.append(f"VECTORS {name} double\n")
+                    out += [f"{f(v[0])} {f(v[1])} {f(v[2])}\n" for v in d]
+                else:
+                    out.append(f"SCALARS {name} double 1\nLOOKUP_TABLE default\n")
+                    out += [f"{f(v[0])}\n" for v in d]
+    return "".join(out).encode()
+
+
+def python_write_vtu_nodal(xyz, conn, pf, cf) -> bytes:
+    """A second restatement of VtkWriter::write_nodal_vtu (vtk_writer.rs:531-789)."""
+    f = rust_display_from_repr
+    head = python_write_vtu(xyz, conn, [], []).decode()
+    head = head[:head.index("    </Piece>")]
+    n = xyz.shape[0]
+    cells = {name: np.asarray(data, np.float64) for name, data, comps in cf if comps == 1}
+    nodal = {k: np.zeros(n) for k in NODAL_NAMES}
+    count = np.zeros(n, np.int64)
+    for k in NODAL_NAMES:
+        if k not in cells:
+            continue
+        for e in range(conn.shape[0]):  # element order, as the reference
+            for node in conn[e]:
+                nodal[k][node] += cells[k][e]
+                if k == "PlasticStrain":
+                    count[node] += 1
+    for k in NODAL_NAMES:
+        nodal[k] = np.where(count > 0, nodal[k] / np.maximum(count, 1), nodal[k])
+    out = [head, "      <PointData>\n"]
+    for name, data, comps in pf:
+        if comps == 3:
+            out.append(f'        <DataArray type="Float64" Name="{name}" NumberOfComponents="3" format="ascii">\n')
+            out += [f"          {f(v[0])} {f(v[1])} {f(v[2])}\n" for v in np.asarray(data, np.float64).reshape(-1, 3)]
+            out.append("        </DataArray>\n")
+    scalars = [(name, data) for name, data, comps in pf if comps == 1] + [(k, nodal[k]) for k in NODAL_NAMES]
+    for name, data in scalars:
+        out.append(f'        <DataArray type="Float64" Name="{name}" format="ascii">\n          ')
+        out += [f(v) + " " for v in np.asarray(data, np.float64).reshape(-1)]
+        out.append("\n        </DataArray>\n")
+    out += ["      </PointData>\n", "    </Piece>\n", "  </UnstructuredGrid>\n", "</VTKFile>\n"]
+    return "".join(out).encode()
+
+
+def golden_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden_vtu", os.path.join(HERE, "golden", "make_golden_vtu.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def golden_inputs(orc):
     import importlib.util
     spec = importlib.util.spec_from_file_location("make_golden_vtu", os.path.join(HERE, "golden", "make_golden_vtu.py"))
@@ -146,6 +220,37 @@ def test_oracle_writer_matches_python_restatement_and_golden(orc):
     bare = orc.write_vtu(xyz, conn)
     assert b"PointData" not in bare and b"CellData" not in bare
     assert bare == python_write_vtu(xyz, conn, [], [])
+
+
+def test_oracle_legacy_and_nodal_writers(orc):
+    """VtkWriter::write and write_nodal_vtu: the oracle = a Python restatement = the golden files."""
+    xyz, conn, pf, cf = golden_inputs(orc)
+    plastic = golden_module().plastic_fields(conn.shape[0])
+    legacy = orc.write_vtu(xyz, conn, pf, cf, fmt="legacy")
+    assert legacy == python_write_vtk(xyz, conn, pf, cf)
+    with open(os.path.join(HERE, "golden", "vtk_2x1x1.vtk"), "rb") as fh:
+        assert fh.read() == legacy
+    nodal = orc.write_vtu(xyz, conn, pf, cf + plastic, fmt="nodal")
+    assert nodal == python_write_vtu_nodal(xyz, conn, pf, cf + plastic)
+    with open(os.path.join(HERE, "golden", "vtu_nodal_2x1x1.vtu"), "rb") as fh:
+        assert fh.read() == nodal
+    # without PlasticStrain the reference leaves the other fields as sums (no count)
+    assert orc.write_vtu(xyz, conn, pf, plastic[1:], fmt="nodal") == python_write_vtu_nodal(xyz, conn, pf,
+                                                                                              plastic[1:])
+    assert orc.write_vtu(xyz, conn, [], [], fmt="legacy") == python_write_vtk(xyz, conn, [], [])
+
+
+def test_vtk_format_and_builder(geo):
+    """vtk_writer.rs:1014-1075 (extension, format detection, recommended filename)."""
+    F = geo.VtkFormat
+    assert [F.extension(f) for f in (F.Legacy, F.Xml, F.XmlNodal, F.XmlMultiBlock)] == [".vtk", ".vtu", ".vtu", ".vtm"]
+    assert F.from_filename("out/a.vtk") == F.Legacy and F.from_filename("a.vtu") == F.XmlNodal
+    assert F.from_filename("a.vtm") == F.XmlMultiBlock and F.from_filename("a.txt") is None
+    b = geo.VtkOutputBuilder(None)
+    assert b.recommended_filename("out/step_0001") == "out/step_0001.vtu"
+    assert b.with_format(F.Legacy).recommended_filename("x") == "x.vtk"
+    b2 = geo.VtkOutputBuilder(None).with_tracers(object()).with_format(F.Legacy).with_fields(["T", "u"])
+    assert b2.format == F.Legacy and b2.tracers is not None and len(b2.fields) == 2
 
 
 def test_python_field_containers(geo):
@@ -230,3 +335,52 @@ def test_device_vtu_streams_many_chunks_and_round_trips(geo, tmp_path):
     assert np.array_equal(ids, dm.elements.reshape(-1))
     temp = np.array(parts[4].split(b'format="ascii">\n', 1)[1].split(), np.float64)
     assert np.array_equal(temp.view(np.uint64), T.view(np.uint64))
+
+
+@pytest.mark.gpu
+def test_device_legacy_and_nodal_match_golden_and_oracle(orc, geo, tmp_path):
+    xyz, conn, pf, cf = golden_inputs(orc)
+    plastic = golden_module().plastic_fields(conn.shape[0])
+    mesh = geo.Mesh(xyz, conn.astype(np.int32))
+    attach(geo, mesh, pf, cf)
+    with open(os.path.join(HERE, "golden", "vtk_2x1x1.vtk"), "rb") as fh:
+        assert geo.VtkWriter.render_vtu(mesh, fmt=geo._native.GEO_VTK_LEGACY) == fh.read()
+    attach(geo, mesh, [], plastic)
+    nodal = geo.VtkWriter.render_vtu(mesh, fmt=geo._native.GEO_VTK_XML_NODAL)
+    with open(os.path.join(HERE, "golden", "vtu_nodal_2x1x1.vtu"), "rb") as fh:
+        assert nodal == fh.read()
+    # the builder's default format and quick_write_vtu write the nodal file
+    path = tmp_path / "step.vtu"
+    assert geo.quick_write_vtu(mesh, str(path)) == len(nodal)
+    assert path.read_bytes() == nodal
+    legacy = tmp_path / "step.vtk"
+    geo.VtkOutputBuilder(mesh).auto_format(str(legacy)).write(str(legacy))
+    assert legacy.read_bytes() == orc.write_vtu(xyz, conn, pf, cf + plastic, fmt="legacy")
+    with pytest.raises(geo.GeoError):
+        geo.VtkOutputBuilder(mesh).with_format(geo.VtkFormat.XmlMultiBlock).write(str(tmp_path / "x.vtm"))
+
+
+@pytest.mark.gpu
+def test_device_nodal_averaging_larger_mesh(orc, geo):
+    """8x6x5 device mesh, plasticity fields with and without PlasticStrain (sums vs
+    averages), vector and scalar point fields from device memory."""
+    import torch
+    s = (8, 6, 5, 1000.0, 800.0, 600.0)
+    dm = geo.ImprovedMeshGenerator.generate_cube_device(*s)
+    xyz, conn = orc.generate_cube(*s)
+    rng = np.random.default_rng(41)
+    u = rng.normal(0.0, 1e-3, 3 * xyz.shape[0])
+    T = rng.normal(600.0, 300.0, xyz.shape[0])
+    plastic = golden_module().plastic_fields(conn.shape[0])
+    for with_strain in (True, False):
+        fields = plastic if with_strain else plastic[1:]
+        dm.field_data = geo.FieldData()
+        dm.cell_data = geo.FieldData()
+        dm.field_data.add_vector_field(geo.VectorField.from_dof_vector("u", torch.from_numpy(u).cuda()))
+        dm.field_data.add_field(geo.ScalarField("T", T))
+        for name, data, _ in fields:
+            dm.cell_data.add_field(geo.ScalarField(name, torch.from_numpy(data).cuda()))
+        got = geo.VtkWriter.render_vtu(dm, fmt=geo._native.GEO_VTK_XML_NODAL)
+        assert got == orc.write_vtu(xyz, conn, [("u", u, 3), ("T", T, 1)], fields, fmt="nodal")
+        legacy = geo.VtkWriter.render_vtu(dm, fmt=geo._native.GEO_VTK_LEGACY)
+        assert legacy == orc.write_vtu(xyz, conn, [("u", u, 3), ("T", T, 1)], fields, fmt="legacy")
