@@ -1025,6 +1025,88 @@ class SolverStats:
                    int(s.kernel_launches))
 
 
+class _CsrKrylov:
+    """Shared builder API of BiCGSTAB and GMRES (iterative.rs:150-175, :303-331)."""
+
+    def __init__(self, name):
+        self.max_iterations = 1000
+        self.tolerance = 1e-8
+        self.abs_tolerance = 1e-12
+        self.use_preconditioner = True
+        self.verbose = False
+        self.timeout_seconds = 10.0
+        self.name = name
+
+    def with_max_iterations(self, n):
+        self.max_iterations = int(n)
+        return self
+
+    def with_tolerance(self, t):
+        self.tolerance = float(t)
+        return self
+
+    def with_abs_tolerance(self, t):
+        self.abs_tolerance = float(t)
+        return self
+
+    def with_verbose(self, flag):
+        self.verbose = bool(flag)  # progress printing is not mirrored
+        return self
+
+    def with_preconditioner(self, flag):
+        self.use_preconditioner = bool(flag)
+        return self
+
+    def opts(self) -> N.CgOpts:
+        o = N.default_opts()
+        o.max_iterations = self.max_iterations
+        o.tolerance = self.tolerance
+        o.abs_tolerance = self.abs_tolerance
+        o.use_preconditioner = int(self.use_preconditioner)
+        o.timeout_seconds = self.timeout_seconds
+        return o
+
+    def _solve(self, fn, A, b, *extra):
+        b = _f64(b)
+        x = np.empty(A.rows()) if isinstance(b, np.ndarray) else b.new_empty(A.rows())
+        st = N.SolverStatsC()
+        o = self.opts()
+        A.ctx.check(fn(A.ctx.h, A.h, _ptr(b), C.byref(o), *extra, _ptr(x), C.byref(st)),
+                    allow=(N.GEO_NOT_CONVERGED, N.GEO_ERR_BREAKDOWN))
+        return x, SolverStats.from_c(st)
+
+
+class BiCGSTAB(_CsrKrylov):
+    """iterative.rs:150-301: right-preconditioned BiCGSTAB on the GPU (FP64, CSR)."""
+
+    def __init__(self):
+        super().__init__("BiCGSTAB")
+
+    new = classmethod(lambda cls: cls())
+
+    def solve(self, A: "CsrMatrix", b):
+        """Solver::solve (iterative.rs:281-288). Returns (x, SolverStats)."""
+        return self._solve(N.lib().geo_bicgstab_solve, A, b)
+
+
+class GMRES(_CsrKrylov):
+    """iterative.rs:303-479: restarted, right-preconditioned GMRES on the GPU (FP64, CSR)."""
+
+    def __init__(self):
+        super().__init__("GMRES")
+        self.restart = 10
+
+    new = classmethod(lambda cls: cls())
+
+    def with_restart(self, m):
+        self.restart = int(m)
+        return self
+
+    def solve(self, A: "CsrMatrix", b):
+        """Solver::solve (iterative.rs:459-466). Returns (x, SolverStats)."""
+        return self._solve(N.lib().geo_gmres_solve, A, b, self.restart)
+
+
 class ConjugateGradient:
     """iterative.rs:7-147: Jacobi-preconditioned CG with the builder API."""
 

@@ -278,6 +278,19 @@ void geo_cg_opts_default(geo_cg_opts* opts);
 int geo_cg_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_opts* opts,
                  double* x, geo_solver_stats* stats);
 
+/* BiCGSTAB::solve (linalg/iterative.rs:150-301) and GMRES::solve (:303-479), the
+ * CG drop-in's siblings: FP64 on the assembled CSR, right-preconditioned with the
+ * Jacobi inverse diagonal (opts->use_preconditioner) or the identity, with the
+ * reference's stopping rules and iteration counting (GMRES counts Arnoldi steps).
+ * opts: max_iterations, tolerance, abs_tolerance, use_preconditioner and
+ * timeout_seconds are used. Returns GEO_NOT_CONVERGED or GEO_ERR_BREAKDOWN (a
+ * |denominator| < 1e-40 in BiCGSTAB) with x and stats valid, as geo_cg_solve.
+ * restart: the GMRES cycle length, 1..64 (the reference's default is 10).      */
+int geo_bicgstab_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_opts* opts, double* x,
+                       geo_solver_stats* stats);
+int geo_gmres_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_opts* opts, int32_t restart,
+                    double* x, geo_solver_stats* stats);
+
 /* No counterpart in the reference. geo_cg_solve without any device allocation, for
  * callers that must not call cudaMalloc/cudaFree between solves (device memory
  * held by another allocator; loops that cannot take cudaFree's device-wide sync).

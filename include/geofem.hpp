@@ -14,6 +14,7 @@
 //   IsotropicElasticity::new(E, nu)                    geofem::IsotropicElasticity{E, nu}
 //   ConjugateGradient::new().with_*(..), Solver::solve geofem::ConjugateGradient().with_*(..).solve(A, b)
 //     (src/linalg/iterative.rs:7-147)
+//   BiCGSTAB / GMRES (src/linalg/iterative.rs:150-479) geofem::BiCGSTAB / GMRES
 //   SolverStats (src/linalg/solver.rs:5-32)            geofem::SolverStats
 //   CsMat<f64> (sprs)                                  geofem::CsMat (device-resident CSR)
 //   FieldData / ScalarField / VectorField (mesh/fields.rs) geofem::FieldData / ScalarField / VectorField
@@ -580,6 +581,52 @@ public:
 
 private:
     geo_cg_opts o_;
+};
+
+// BiCGSTAB (iterative.rs:150-301) and restarted GMRES (:303-479) on the assembled
+// CSR, FP64, right-preconditioned with Jacobi or the identity
+class BiCGSTAB {
+public:
+    BiCGSTAB() { geo_cg_opts_default(&o_); }
+    BiCGSTAB& with_max_iterations(int64_t n) { o_.max_iterations = n; return *this; }
+    BiCGSTAB& with_tolerance(double t) { o_.tolerance = t; return *this; }
+    BiCGSTAB& with_abs_tolerance(double t) { o_.abs_tolerance = t; return *this; }
+    BiCGSTAB& with_preconditioner(bool on) { o_.use_preconditioner = on ? 1 : 0; return *this; }
+    std::pair<std::vector<double>, SolverStats> solve(const CsMat& A, const std::vector<double>& b) const {
+        Context& ctx = *A.context();
+        if ((int64_t)b.size() != A.rows()) throw Error(GEO_ERR_INVALID_ARG, "b has the wrong length");
+        std::vector<double> x(b.size());
+        geo_solver_stats st{};
+        ctx.check(geo_bicgstab_solve(ctx.get(), A.get(), b.data(), &o_, x.data(), &st),
+                  {GEO_NOT_CONVERGED, GEO_ERR_BREAKDOWN});
+        return {std::move(x), SolverStats::from_c(st)};
+    }
+
+private:
+    geo_cg_opts o_;
+};
+
+class GMRES {
+public:
+    GMRES() { geo_cg_opts_default(&o_); }
+    GMRES& with_restart(int m) { restart_ = m; return *this; }
+    GMRES& with_max_iterations(int64_t n) { o_.max_iterations = n; return *this; }
+    GMRES& with_tolerance(double t) { o_.tolerance = t; return *this; }
+    GMRES& with_abs_tolerance(double t) { o_.abs_tolerance = t; return *this; }
+    GMRES& with_preconditioner(bool on) { o_.use_preconditioner = on ? 1 : 0; return *this; }
+    std::pair<std::vector<double>, SolverStats> solve(const CsMat& A, const std::vector<double>& b) const {
+        Context& ctx = *A.context();
+        if ((int64_t)b.size() != A.rows()) throw Error(GEO_ERR_INVALID_ARG, "b has the wrong length");
+        std::vector<double> x(b.size());
+        geo_solver_stats st{};
+        ctx.check(geo_gmres_solve(ctx.get(), A.get(), b.data(), &o_, restart_, x.data(), &st),
+                  {GEO_NOT_CONVERGED, GEO_ERR_BREAKDOWN});
+        return {std::move(x), SolverStats::from_c(st)};
+    }
+
+private:
+    geo_cg_opts o_;
+    int restart_ = 10;  // the reference's default
 };
 
 // ---------------------------------------------------------------- matrix-free operators

@@ -859,6 +859,188 @@ void orc_cg_solve(const orc_csr* A, const double* b, int64_t max_iterations, dou
                     elapsed()};
 }
 
+// Jacobi (preconditioner.rs:37-62) or identity inverse diagonal
+static std::vector<double> jacobi_inverse(const orc_csr* A, int use_preconditioner) {
+    std::vector<double> d((size_t)A->rows, 1.0);
+    if (use_preconditioner)
+        for (int64_t i = 0; i < A->rows; ++i) {
+            bool found;
+            const double v = csr_get(A, i, i, &found);
+            if (found && std::fabs(v) > 1e-14) d[(size_t)i] = 1.0 / v;
+        }
+    return d;
+}
+
+static double dot(const std::vector<double>& a, const std::vector<double>& b) {
+    double s = 0.0;
+    for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+    return s;
+}
+
+// BiCGSTAB::solve_with_operator_internal (iterative.rs:177-278), right-preconditioned
+void orc_bicgstab_solve(const orc_csr* A, const double* b, int64_t max_iterations, double tolerance,
+                        double abs_tolerance, int use_preconditioner, double* x_out, orc_stats* st) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const int64_t n = A->rows;
+    const std::vector<double> dinv = jacobi_inverse(A, use_preconditioner);
+    auto elapsed = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    std::vector<double> bv(b, b + n);
+    const double b_norm = norm2(bv);
+    if (b_norm < 1e-25) {
+        for (int64_t i = 0; i < n; ++i) x_out[i] = 0.0;
+        *st = orc_stats{0, 0.0, 0.0, 1, elapsed()};
+        return;
+    }
+    std::vector<double> x(n, 0.0), r = bv, r_hat = bv, v(n, 0.0), p(n, 0.0), p_hat(n), s(n), s_hat(n), t(n);
+    double rho = 1.0, alpha = 1.0, omega = 1.0, final_res = b_norm;
+    int64_t total = 0;
+    bool converged = false;
+    while (total < max_iterations) {
+        const double rho_prev = rho;
+        rho = dot(r_hat, r);
+        if (std::fabs(rho) < 1e-40) break;
+        if (total == 0) {
+            p = r;
+        } else {
+            const double beta = (rho / rho_prev) * (alpha / omega);
+            for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+        }
+        for (int64_t i = 0; i < n; ++i) p_hat[i] = p[i] * dinv[i];
+        orc_csr_apply(A, p_hat.data(), v.data());
+        const double rhat_v = dot(r_hat, v);
+        if (std::fabs(rhat_v) < 1e-40) break;
+        alpha = rho / rhat_v;
+        for (int64_t i = 0; i < n; ++i) s[i] = r[i] - alpha * v[i];
+        const double s_norm = norm2(s);
+        if (s_norm < tolerance * b_norm || s_norm < abs_tolerance) {
+            for (int64_t i = 0; i < n; ++i) x[i] += alpha * p_hat[i];
+            final_res = s_norm;
+            converged = true;
+            break;
+        }
+        for (int64_t i = 0; i < n; ++i) s_hat[i] = s[i] * dinv[i];
+        orc_csr_apply(A, s_hat.data(), t.data());
+        const double t_t = dot(t, t), t_s = dot(t, s);
+        if (std::fabs(t_t) < 1e-40) break;
+        omega = t_s / t_t;
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] += alpha * p_hat[i] + omega * s_hat[i];
+            r[i] = s[i] - omega * t[i];
+        }
+        final_res = norm2(r);
+        total += 1;
+        if (final_res < tolerance * b_norm || final_res < abs_tolerance) {
+            converged = true;
+            break;
+        }
+        if (std::fabs(omega) < 1e-40) break;
+    }
+    for (int64_t i = 0; i < n; ++i) x_out[i] = x[i];
+    *st = orc_stats{total, final_res, final_res / b_norm, converged ? 1 : 0, elapsed()};
+}
+
+// GMRES::solve_with_operator_internal (iterative.rs:333-456): restarted, right-
+// preconditioned, modified Gram-Schmidt, Givens rotations (givens_rotation, :458-467)
+void orc_gmres_solve(const orc_csr* A, const double* b, int64_t max_iterations, int64_t restart, double tolerance,
+                     double abs_tolerance, int use_preconditioner, double* x_out, orc_stats* st) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const int64_t n = A->rows;
+    const std::vector<double> dinv = jacobi_inverse(A, use_preconditioner);
+    auto elapsed = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    std::vector<double> bv(b, b + n);
+    const double b_norm = norm2(bv);
+    if (b_norm < 1e-25) {
+        for (int64_t i = 0; i < n; ++i) x_out[i] = 0.0;
+        *st = orc_stats{0, 0.0, 0.0, 1, elapsed()};
+        return;
+    }
+    auto givens = [](double a, double bb, double& c, double& s, double& rho) {
+        if (std::fabs(bb) < 1e-40) {
+            c = 1.0;
+            s = 0.0;
+            rho = a;
+        } else if (std::fabs(bb) > std::fabs(a)) {
+            const double tau = a / bb;
+            s = 1.0 / std::sqrt(1.0 + tau * tau);
+            c = s * tau;
+            rho = bb * std::sqrt(1.0 + tau * tau);
+        } else {
+            const double tau = bb / a;
+            c = 1.0 / std::sqrt(1.0 + tau * tau);
+            s = c * tau;
+            rho = a * std::sqrt(1.0 + tau * tau);
+        }
+    };
+    std::vector<double> x(n, 0.0), r(n), w(n), z(n);
+    int64_t total = 0;
+    bool converged = false;
+    double final_res = b_norm;
+    const int64_t m = restart;
+    while (total < max_iterations) {
+        orc_csr_apply(A, x.data(), r.data());  // r = b - A x
+        for (int64_t i = 0; i < n; ++i) r[i] = bv[i] - r[i];
+        const double r_norm = norm2(r);
+        final_res = r_norm;
+        if (r_norm < tolerance * b_norm || r_norm < abs_tolerance) {
+            converged = true;
+            break;
+        }
+        std::vector<std::vector<double>> v((size_t)m + 1, std::vector<double>(n, 0.0));
+        std::vector<std::vector<double>> h((size_t)m + 1, std::vector<double>((size_t)m, 0.0));
+        for (int64_t i = 0; i < n; ++i) v[0][i] = r[i] / r_norm;
+        std::vector<double> g((size_t)m + 1, 0.0), cs((size_t)m, 0.0), sn((size_t)m, 0.0);
+        g[0] = r_norm;
+        int64_t k = 0;
+        for (int64_t j = 0; j < m; ++j) {
+            if (total >= max_iterations) break;
+            for (int64_t i = 0; i < n; ++i) z[i] = v[j][i] * dinv[i];
+            orc_csr_apply(A, z.data(), w.data());
+            for (int64_t i = 0; i <= j; ++i) {
+                h[i][j] = dot(v[i], w);
+                for (int64_t l = 0; l < n; ++l) w[l] -= h[i][j] * v[i][l];
+            }
+            h[j + 1][j] = norm2(w);
+            if (std::fabs(h[j + 1][j]) > 1e-40)
+                for (int64_t l = 0; l < n; ++l) v[j + 1][l] = w[l] / h[j + 1][j];
+            for (int64_t i = 0; i < j; ++i) {
+                const double temp = cs[i] * h[i][j] + sn[i] * h[i + 1][j];
+                h[i + 1][j] = -sn[i] * h[i][j] + cs[i] * h[i + 1][j];
+                h[i][j] = temp;
+            }
+            double c, s, rho;
+            givens(h[j][j], h[j + 1][j], c, s, rho);
+            cs[j] = c;
+            sn[j] = s;
+            h[j][j] = rho;
+            h[j + 1][j] = 0.0;
+            const double temp = cs[j] * g[j];
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = temp;
+            k = j + 1;
+            total += 1;
+            final_res = std::fabs(g[k]);
+            if (final_res < tolerance * b_norm || final_res < abs_tolerance) break;
+        }
+        std::vector<double> y((size_t)k, 0.0);
+        for (int64_t i = k - 1; i >= 0; --i) {
+            double sum = 0.0;
+            for (int64_t j = i + 1; j < k; ++j) sum += h[i][j] * y[j];
+            if (std::fabs(h[i][i]) < 1e-40) break;
+            y[i] = (g[i] - sum) / h[i][i];
+        }
+        std::vector<double> dy(n, 0.0);
+        for (int64_t j = 0; j < k; ++j)
+            for (int64_t i = 0; i < n; ++i) dy[i] += v[j][i] * y[j];
+        for (int64_t i = 0; i < n; ++i) x[i] += dy[i] * dinv[i];
+        if (final_res < tolerance * b_norm || final_res < abs_tolerance) {
+            converged = true;
+            break;
+        }
+    }
+    for (int64_t i = 0; i < n; ++i) x_out[i] = x[i];
+    *st = orc_stats{total, final_res, final_res / b_norm, converged ? 1 : 0, elapsed()};
+}
+
 // direct.rs:28-73: dense LU with partial pivoting; converged <=> rel-res < 1e-8
 int orc_lu_solve(const orc_csr* A, const double* b, double* x, orc_stats* st) {
     const auto t0 = std::chrono::steady_clock::now();

@@ -96,6 +96,11 @@ void orc_csr_apply(const orc_csr* A, const double* x, double* y);
 void orc_csr_free(orc_csr* A);
 
 /* ---- solvers: iterative.rs:46-131, preconditioner.rs:37-72, direct.rs:28-73 ---- */
+/* iterative.rs:177-278 (BiCGSTAB) and :333-456 (GMRES(restart)), same stats as orc_cg_solve */
+void orc_bicgstab_solve(const orc_csr* A, const double* b, int64_t max_iterations, double tolerance,
+                        double abs_tolerance, int use_preconditioner, double* x_out, orc_stats* st);
+void orc_gmres_solve(const orc_csr* A, const double* b, int64_t max_iterations, int64_t restart, double tolerance,
+                     double abs_tolerance, int use_preconditioner, double* x_out, orc_stats* st);
 void orc_cg_solve(const orc_csr* A, const double* b, int64_t max_iterations, double tolerance,
                   double abs_tolerance, int use_preconditioner, double* x, orc_stats* stats);
 int orc_lu_solve(const orc_csr* A, const double* b, double* x, orc_stats* stats);

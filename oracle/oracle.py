@@ -92,6 +92,10 @@ def _declare(L):
         "orc_cg_solve": (None, [_P, _D, C.c_int64, C.c_double, C.c_double, C.c_int, _D,
                                 C.POINTER(OrcStats)]),
         "orc_lu_solve": (C.c_int, [_P, _D, _D, C.POINTER(OrcStats)]),
+        "orc_bicgstab_solve": (None, [_P, _D, C.c_int64, C.c_double, C.c_double, C.c_int, _D,
+                                      C.POINTER(OrcStats)]),
+        "orc_gmres_solve": (None, [_P, _D, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int, _D,
+                                   C.POINTER(OrcStats)]),
         "orc_thermal_element_gradient": (None, [C.c_int64, _D, C.c_int64, _I64, _D, _D, _D, _D]),
         "orc_elasticity_element_gradient": (None, [C.c_int64, _D, C.c_int64, _I64, _D, C.c_double,
                                                    _D, _D, _D]),
@@ -408,6 +412,30 @@ def cg_solve(A: Csr, b, max_iterations=1000, tolerance=1e-8, abs_tolerance=1e-12
     st = OrcStats()
     lib().orc_cg_solve(h, _d(_f64(b)), int(max_iterations), tolerance, abs_tolerance,
                        int(bool(use_preconditioner)), _d(x), C.byref(st))
+    lib().orc_csr_free(h)
+    return x, st
+
+
+def bicgstab_solve(A: Csr, b, max_iterations=1000, tolerance=1e-8, abs_tolerance=1e-12,
+                   use_preconditioner=True):
+    """BiCGSTAB::solve (iterative.rs:177-278)."""
+    h = A.handle()
+    x = np.empty(A.n_rows)
+    st = OrcStats()
+    lib().orc_bicgstab_solve(h, _d(_f64(b)), int(max_iterations), tolerance, abs_tolerance,
+                             int(bool(use_preconditioner)), _d(x), C.byref(st))
+    lib().orc_csr_free(h)
+    return x, st
+
+
+def gmres_solve(A: Csr, b, max_iterations=1000, restart=10, tolerance=1e-8, abs_tolerance=1e-12,
+                use_preconditioner=True):
+    """GMRES::solve (iterative.rs:333-456)."""
+    h = A.handle()
+    x = np.empty(A.n_rows)
+    st = OrcStats()
+    lib().orc_gmres_solve(h, _d(_f64(b)), int(max_iterations), int(restart), tolerance, abs_tolerance,
+                          int(bool(use_preconditioner)), _d(x), C.byref(st))
     lib().orc_csr_free(h)
     return x, st
 

@@ -231,6 +231,17 @@ void errors() {
            "max_iterations reached: converged = false, no exception");
 }
 
+// The reference's 2x2 system (iterative.rs:491-504) through the CG siblings
+void krylov_siblings() {
+    const CsMat A = CsMat::from_arrays(2, 2, {0, 2, 4}, {0, 1, 0, 1}, {2.0, 1.0, 1.0, 2.0});
+    const auto bi = BiCGSTAB().solve(A, {3.0, 3.0});
+    const auto gm = GMRES().with_restart(5).solve(A, {3.0, 3.0});
+    expect(bi.second.converged && std::fabs(bi.first[0] - 1.0) < 1e-6 && std::fabs(bi.first[1] - 1.0) < 1e-6,
+           "BiCGSTAB on the 2x2 system");
+    expect(gm.second.converged && std::fabs(gm.first[0] - 1.0) < 1e-6 && std::fabs(gm.first[1] - 1.0) < 1e-6,
+           "GMRES on the 2x2 system");
+}
+
 void adjoint_fd() {
     const double lz = 600;
     Mesh mesh = ImprovedMeshGenerator::generate_cube(4, 4, 3, 1000, 1000, lz);
@@ -357,6 +368,7 @@ int main() {
         maxwell_relaxation();
         errors();
         adjoint_fd();
+        krylov_siblings();
         device_mesh();
         vtu_output();
     } catch (const Error& e) {
