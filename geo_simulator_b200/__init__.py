@@ -11,7 +11,7 @@ from .fem import (  # noqa: F401
     ElasticityElement, ElasticityOperator, ElementMatrix, GeoError, ImprovedMeshGenerator, IsotropicElasticity,
     MaxwellViscoelasticity, Mesh, DeviceMesh, NeumannBC, SolverStats, StressHistory, Tet10Face, ThermalOperator, BackwardEuler,
     TimeStepStats, update_stresses_maxwell, FieldData, ScalarField, VectorField, VtkWriter,
-    VtkFormat, VtkOutputBuilder, quick_write_vtu, BiCGSTAB, GMRES,
+    VtkFormat, VtkOutputBuilder, quick_write_vtu, BiCGSTAB, GMRES, DirectSolver,
 )
 
 __version__ = "0.1.0"

@@ -24,6 +24,7 @@ GEO_ERR_CUDA = 6
 GEO_ERR_UNSUPPORTED = 7
 GEO_ERR_NO_DEVICE = 8
 GEO_ERR_OUT_OF_MEMORY = 9
+GEO_ERR_SINGULAR_MATRIX = 10
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -31,7 +32,7 @@ PRECISION_MIXED = 1
 STATUS_NAMES = {
     0: "GEO_OK", 1: "GEO_ERR_INVALID_ARG", 2: "GEO_ERR_SINGULAR_JACOBIAN", 3: "GEO_NOT_CONVERGED",
     4: "GEO_ERR_BREAKDOWN", 5: "GEO_ERR_TIMEOUT", 6: "GEO_ERR_CUDA", 7: "GEO_ERR_UNSUPPORTED",
-    8: "GEO_ERR_NO_DEVICE", 9: "GEO_ERR_OUT_OF_MEMORY",
+    8: "GEO_ERR_NO_DEVICE", 9: "GEO_ERR_OUT_OF_MEMORY", 10: "GEO_ERR_SINGULAR_MATRIX",
 }
 
 
@@ -100,6 +101,7 @@ _SIGS = {
     "geo_cg_solve": [_P, _P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_bicgstab_solve": [_P, _P, _DP, C.POINTER(CgOpts), _DP, C.POINTER(SolverStatsC)],
     "geo_gmres_solve": [_P, _P, _DP, C.POINTER(CgOpts), _I32, _DP, C.POINTER(SolverStatsC)],
+    "geo_direct_solve": [_P, _P, _DP, _DP, C.POINTER(SolverStatsC)],
     "geo_thermal_operator_create": [_P, _P, _P, _DP, _D, _PP],
     "geo_elasticity_operator_create": [_P, _P, _P, _DP, _D, _D, _PP],
     "geo_op_set_coefficients": [_P, _DP, _D],

@@ -1107,6 +1107,42 @@ class GMRES(_CsrKrylov):
         return self._solve(N.lib().geo_gmres_solve, A, b, self.restart)
 
 
+class DirectSolver:
+    """direct.rs:9-95: dense LU with partial pivoting on the GPU (FP64); no iterations."""
+
+    def __init__(self):
+        self.name = "Direct (Sparse LU)"
+
+    new = classmethod(lambda cls: cls())
+
+    def solve(self, A: "CsrMatrix", b):
+        """Solver::solve (direct.rs:28-73). Returns (x, SolverStats); a singular
+        matrix raises GeoError(GEO_ERR_SINGULAR_MATRIX), where the reference panics."""
+        b = _f64(b)
+        x = np.empty(A.rows()) if isinstance(b, np.ndarray) else b.new_empty(A.rows())
+        st = N.SolverStatsC()
+        A.ctx.check(N.lib().geo_direct_solve(A.ctx.h, A.h, _ptr(b), _ptr(x), C.byref(st)))
+        return x, SolverStats.from_c(st)
+
+    def solve_with_operator(self, A, b, precond=None):
+        """direct.rs:75-86: the direct solver needs an assembled matrix."""
+        raise N.GeoError(N.GEO_ERR_UNSUPPORTED,
+                         "DirectSolver does not support matrix-free operator. Use iterative solvers instead.")
+
+    # direct.rs:92-95: the tolerances are fixed at 0 and the setters do nothing
+    def tolerance(self):
+        return 0.0
+
+    def abs_tolerance(self):
+        return 0.0
+
+    def set_tolerance(self, t):
+        pass
+
+    def set_abs_tolerance(self, t):
+        pass
+
+
 class ConjugateGradient:
     """iterative.rs:7-147: Jacobi-preconditioned CG with the builder API."""
 

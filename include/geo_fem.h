@@ -48,6 +48,7 @@ extern "C" {
 #define GEO_ERR_UNSUPPORTED 7
 #define GEO_ERR_NO_DEVICE 8
 #define GEO_ERR_OUT_OF_MEMORY 9
+#define GEO_ERR_SINGULAR_MATRIX 10   /* direct.rs:52 `expect("LU solve failed")` */
 
 /* precision of the matrix-free solver (geo_cg_opts.precision) */
 #define GEO_PRECISION_FP64 0  /* plain FP64 throughout (the drop-in semantics)           */
@@ -290,6 +291,15 @@ int geo_bicgstab_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const ge
                        geo_solver_stats* stats);
 int geo_gmres_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_opts* opts, int32_t restart,
                     double* x, geo_solver_stats* stats);
+
+/* DirectSolver::solve (linalg/direct.rs:28-73): the CSR matrix densified on the
+ * device and solved by LU with partial pivoting (first row of largest |a_ik|, as
+ * the reference's dense LU), FP64, in one persistent cooperative kernel.
+ * n_rows <= 16384 (the dense factor takes 8 n^2 bytes; else GEO_ERR_INVALID_ARG).
+ * A zero pivot returns GEO_ERR_SINGULAR_MATRIX (the reference panics, "LU solve
+ * failed"). stats: iterations 0, residual_norm ||b - A x||, relative_residual
+ * (solver.rs:165-175), converged = relative_residual < 1e-8 (direct.rs:58-66). */
+int geo_direct_solve(geo_ctx* ctx, const geo_csr* A, const double* b, double* x, geo_solver_stats* stats);
 
 /* No counterpart in the reference. geo_cg_solve without any device allocation, for
  * callers that must not call cudaMalloc/cudaFree between solves (device memory

@@ -606,6 +606,26 @@ private:
     geo_cg_opts o_;
 };
 
+// DirectSolver (linalg/direct.rs:9-95): dense LU with partial pivoting on the
+// device. A singular matrix throws Error(GEO_ERR_SINGULAR_MATRIX), where the
+// reference panics; the tolerances are fixed at 0 as there.
+class DirectSolver {
+public:
+    std::pair<std::vector<double>, SolverStats> solve(const CsMat& A, const std::vector<double>& b) const {
+        Context& ctx = *A.context();
+        if ((int64_t)b.size() != A.rows()) throw Error(GEO_ERR_INVALID_ARG, "b has the wrong length");
+        std::vector<double> x(b.size());
+        geo_solver_stats st{};
+        ctx.check(geo_direct_solve(ctx.get(), A.get(), b.data(), x.data(), &st));
+        return {std::move(x), SolverStats::from_c(st)};
+    }
+    const char* name() const { return "Direct (Sparse LU)"; }
+    double tolerance() const { return 0.0; }
+    double abs_tolerance() const { return 0.0; }
+    void set_tolerance(double) {}
+    void set_abs_tolerance(double) {}
+};
+
 class GMRES {
 public:
     GMRES() { geo_cg_opts_default(&o_); }

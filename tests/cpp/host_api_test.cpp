@@ -240,6 +240,19 @@ void krylov_siblings() {
            "BiCGSTAB on the 2x2 system");
     expect(gm.second.converged && std::fabs(gm.first[0] - 1.0) < 1e-6 && std::fabs(gm.first[1] - 1.0) < 1e-6,
            "GMRES on the 2x2 system");
+    // direct.rs:103-122
+    const auto lu = DirectSolver().solve(A, {3.0, 3.0});
+    expect(lu.second.converged && lu.second.iterations == 0 && std::fabs(lu.first[0] - 1.0) < 1e-10 &&
+               std::fabs(lu.first[1] - 1.0) < 1e-10,
+           "DirectSolver on the 2x2 system");
+    const CsMat S = CsMat::from_arrays(2, 2, {0, 2, 4}, {0, 1, 0, 1}, {1.0, 2.0, 2.0, 4.0});
+    bool singular = false;
+    try {
+        DirectSolver().solve(S, {1.0, 1.0});
+    } catch (const Error& e) {
+        singular = e.code() == GEO_ERR_SINGULAR_MATRIX;
+    }
+    expect(singular, "DirectSolver raises GEO_ERR_SINGULAR_MATRIX on a singular matrix");
 }
 
 void adjoint_fd() {
