@@ -130,7 +130,9 @@ int geo_ctx_destroy(geo_ctx* ctx) {
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    const int dev = ctx->device;
     delete ctx;
+    geo::dev_release_cached(dev);
     return GEO_OK;
 }
 

@@ -43,6 +43,17 @@ enum : int {
     DEV_ERR_BOUNDS = 4,
 };
 
+// ------------------------------------------------------------------ device memory
+// Caching allocator behind every DevBuf (devmem.cu). A freed block goes back to a
+// per-device cache once the device has finished the work queued before the free
+// (the wait cudaFree implies, without its unmapping) and is handed out again for a
+// request of the same rounded size, so objects created and destroyed call after
+// call stop paying cudaMalloc / cudaFree. A cudaMalloc that runs out of memory
+// releases the device's cache and is retried once.
+void* dev_alloc(size_t bytes);
+void dev_free(void* p) noexcept;
+void dev_release_cached(int device);  // device < 0: every device
+
 // ------------------------------------------------------------------ buffers
 template <class T>
 struct DevBuf {
@@ -61,7 +72,7 @@ struct DevBuf {
     void alloc(size_t count) {
         release();
         if (count == 0) return;
-        GEO_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        p = static_cast<T*>(dev_alloc(count * sizeof(T)));
         n = count;
     }
     // grow-only reallocation for workspaces
@@ -69,7 +80,7 @@ struct DevBuf {
         if (count > n) alloc(count);
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         n = 0;
     }

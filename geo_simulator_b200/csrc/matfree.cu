@@ -8,11 +8,15 @@
 // patch's nodal values into shared memory, every thread applies K_e of its
 // elements from the per-element qdata, accumulates into shared memory, and the
 // patch flushes its nodes: plain stores for nodes no other patch touches,
-// red.global.add for the shared ones (so the matrix-free result is not
-// bit-reproducible in the last bit; the assembled path is).
+// red.global.add for the shared ones (so the matrix-free apply is not
+// bit-reproducible in the last bit; the assembled path is). The PCG of a one-DOF
+// operator runs in halo mode instead: foreign contributions are stored to
+// per-entry slots and added by the node update in slot order, with no atomics.
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
+
+#include <cub/cub.cuh>
 
 #include "mf_kernels.cuh"
 #include "pcg_common.cuh"
@@ -175,6 +179,42 @@ __global__ void k_patch_foreign(const int32_t* __restrict__ pf, const int32_t* _
         const int32_t nd = foreign[f0 + k];
         fids[a0 + k] = nd;
         fflags[a0 + k] = flags[nd];
+    }
+}
+
+// Halo slots of a one-DOF operator's PCG: every foreign entry a (patch p, its
+// k-th foreign node n, a = pf[p] + k) gets a slot. Slots are ordered by node n,
+// then by entry (a stable sort of the entries by node), so node n's slots are
+// consecutive and follow those of the nodes before it.
+__global__ void k_halo_count(const int32_t* __restrict__ foreign, int64_t n_app, int32_t* __restrict__ cnt) {
+    for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < n_app; a += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[foreign[a]], 1);
+}
+__global__ void k_iota(int64_t n, int32_t* __restrict__ v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = (int32_t)i;
+}
+__global__ void k_halo_slot_of(const int32_t* __restrict__ sorted_app, int64_t n_app, int32_t* __restrict__ slot_of) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_app; t += (int64_t)gridDim.x * blockDim.x)
+        slot_of[sorted_app[t]] = (int32_t)t;
+}
+// the slots again in the per-patch segments of fids (one block per patch)
+__global__ void k_patch_fslot(const int32_t* __restrict__ pf, const int32_t* __restrict__ pfa,
+                              const int32_t* __restrict__ slot_of, int32_t* __restrict__ fslot) {
+    const int p = blockIdx.x;
+    const int f0 = pf[p], nf = pf[p + 1] - f0, a0 = pfa[p];
+    for (int k = threadIdx.x; k < nf; k += blockDim.x) fslot[a0 + k] = slot_of[f0 + k];
+}
+// flag bits 3-6 = slot count (<= 15); chunk[c] = slots of nodes [32 c, 32 c + 32).
+// The grid covers whole warps of 32 consecutive nodes.
+__global__ void k_halo_flags(const int32_t* __restrict__ cnt, int64_t N, uint8_t* __restrict__ flags,
+                             int32_t* __restrict__ chunk) {
+    const int64_t N32 = (N + 31) / 32 * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N32; i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = i < N ? cnt[i] : 0;
+        if (i < N) flags[i] = (uint8_t)(flags[i] | (c << kHaloShift));
+        const int sum = __reduce_add_sync(0xffffffffu, c);
+        if ((threadIdx.x & 31) == 0) chunk[i / 32] = sum;
     }
 }
 
@@ -404,6 +444,14 @@ struct geo_op {
     geo::DevBuf<uint8_t> fflags;
     int max_for = 0;
     int max_own = 0;  // largest own-node count of a patch
+    // halo mode of the PCG (one DOF per node): slot of every foreign entry (fids
+    // segments), slots before each 32-node chunk, and the slot arrays
+    geo::DevBuf<int32_t> fslot, hbase;
+    geo::DevBuf<double> halo64;
+    geo::DevBuf<float> halo32;
+    int64_t n_app = 0;
+    bool halo_ok = false;  // slots built (every node has at most 15)
+    int halo[2] = {0, 0};  // halo mode in use (FP64, FP32), see setup
     // per-patch bound of the fixed-point scatter (Scatter in mf_kernels.cuh)
     geo::DevBuf<int32_t> pmaxinc;
     geo::DevBuf<float> pbound32;
@@ -469,18 +517,21 @@ PatchView view(const geo_op* op) {
     v.max_for = op->max_for;
     v.max_own = op->max_own;
     v.own_bulk = 0;
+    v.fslot = op->fslot.p;
+    v.halo = 0;
     return v;
 }
 
 // dynamic shared memory of the patch kernel: barriers, element-data buffers, node tables
 template <class K, class T>
-size_t smem_bytes(const geo_op* op, int nbuf, bool own) {
+size_t smem_bytes(const geo_op* op, int nbuf, bool own, bool halo = false) {
     // xs (T), fixed-point accumulators (Scatter<T>::kWords INT32 words), flags, and for
     // FP32 thermal PCG the own-node slices
     const size_t tables = (size_t)op->max_local * K::DPN * (sizeof(T) + 4 * Scatter<T>::kWords) +
                           (size_t)op->max_local + 16 +
                           (own ? (size_t)own_bytes<T>(op->max_own, K::DPN) : 0);
-    return (nbuf == 2 ? patch_smem_tables<K, T, 2>(op->max_for) : patch_smem_tables<K, T, 1>(op->max_for)) + tables;
+    return (nbuf == 2 ? patch_smem_tables<K, T, 2>(op->max_for, halo) : patch_smem_tables<K, T, 1>(op->max_for, halo)) +
+           tables;
 }
 
 constexpr size_t kSmemLimit = 227 * 1024;
@@ -538,6 +589,23 @@ int setup_patch_kernels(geo_op* op, int slot) {
     op->own_bulk[slot] = own && per_sm_own >= per_sm;
     op->patch_smem[slot] = op->own_bulk[slot] ? own : plain;
     if (per_sm < 1) fail(GEO_ERR_UNSUPPORTED, "patch kernel does not fit on an SM");
+    per_sm = std::max(per_sm, per_sm_own);
+    // halo mode (one DOF per node) when its slot lists cost no resident block
+    op->halo[slot] = 0;
+    if (K::DPN == 1 && op->halo_ok) {
+        const size_t hs = smem_bytes<K, T>(op, nbuf, op->own_bulk[slot] != 0, true);
+        int per_sm_halo = 0;
+        if (hs <= kSmemLimit) {
+            // raises the limit of every mode's kernel (all launch with patch_smem[slot])
+            const size_t attr = std::max(hs, std::max(plain, own));
+            if (nbuf == 2) setup_patch_nbuf<K, T, 2>(attr, hs, 0, per_sm_halo);
+            else setup_patch_nbuf<K, T, 1>(attr, hs, 0, per_sm_halo);
+        }
+        if (per_sm_halo >= per_sm) {
+            op->halo[slot] = 1;
+            op->patch_smem[slot] = hs;
+        }
+    }
     return per_sm * op->ctx->sm_count;
 }
 
@@ -546,11 +614,66 @@ void launch_patch(const geo_op* op, int slot, cudaStream_t s, const T* qd, const
     const unsigned g = (unsigned)std::min(op->patch_grid[slot], op->n_patches);
     PatchView v = view(op);
     v.own_bulk = op->own_bulk[slot];
+    v.halo = MODE == MODE_PCG ? op->halo[slot] : 0;
     const size_t smem = op->patch_smem[slot];
     if (op->nbuf[slot] == 2)
         k_patch<K, T, MODE, 2><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
     else
         k_patch<K, T, MODE, 1><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
+}
+
+// Halo slots of a one-DOF operator (see k_halo_count): fslot in the fids
+// segments (seg_total entries), the slot counts in flag bits 3-6, hbase, and the
+// FP64 / FP32 slot arrays. Leaves op->halo_ok false (atomics kept) when some node
+// has more than 15 foreign entries.
+void build_halo_slots(geo_op* op, int64_t seg_total) {
+    geo_ctx* ctx = op->ctx;
+    cudaStream_t s = ctx->stream;
+    const int64_t N = op->N, A = op->n_app;
+    DevBuf<int32_t> cnt(N), keys(A), vals(A), vals2(A), slot_of(A), mx(1);
+    GEO_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), s));
+    k_halo_count<<<nblk(A), 256, 0, s>>>(op->foreign.p, A, cnt.p);
+    check_launch(ctx, "k_halo_count");
+    size_t b1 = 0, b2 = 0;
+    int bits = 1;
+    while (bits < 31 && (int64_t(1) << bits) < N) ++bits;
+    GEO_CUDA(cub::DeviceReduce::Max(nullptr, b1, cnt.p, mx.p, N, s));
+    GEO_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b2, op->foreign.p, keys.p, vals.p, vals2.p, A, 0, bits, s));
+    DevBuf<unsigned char> tmp(std::max(b1, b2));
+    GEO_CUDA(cub::DeviceReduce::Max(tmp.p, b1, cnt.p, mx.p, N, s));
+    int hmax = 0;
+    GEO_CUDA(cudaMemcpyAsync(&hmax, mx.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    sync(ctx, "halo counts");
+    if (hmax > 15) return;
+    k_iota<<<nblk(A), 256, 0, s>>>(A, vals.p);
+    check_launch(ctx, "k_iota");
+    GEO_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, b2, op->foreign.p, keys.p, vals.p, vals2.p, A, 0, bits, s));
+    k_halo_slot_of<<<nblk(A), 256, 0, s>>>(vals2.p, A, slot_of.p);
+    check_launch(ctx, "k_halo_slot_of");
+    op->fslot.alloc(seg_total + kForeignAlign);
+    GEO_CUDA(cudaMemsetAsync(op->fslot.p, 0, op->fslot.bytes(), s));
+    k_patch_fslot<<<(unsigned)op->n_patches, 128, 0, s>>>(op->pf.p, op->pfa.p, slot_of.p, op->fslot.p);
+    check_launch(ctx, "k_patch_fslot");
+    const int64_t nch = (N + 31) / 32;
+    DevBuf<int32_t> chunk(nch + 1);
+    GEO_CUDA(cudaMemsetAsync(chunk.p, 0, chunk.bytes(), s));
+    k_halo_flags<<<nblk(nch * 32), 256, 0, s>>>(cnt.p, N, op->flags.p, chunk.p);
+    check_launch(ctx, "k_halo_flags");
+    op->hbase.alloc(nch + 1);
+    size_t b3 = 0;
+    GEO_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b3, chunk.p, op->hbase.p, nch + 1, s));
+    tmp.ensure(b3);
+    GEO_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, b3, chunk.p, op->hbase.p, nch + 1, s));
+    int total = 0;
+    GEO_CUDA(cudaMemcpyAsync(&total, op->hbase.p + nch, sizeof(int), cudaMemcpyDeviceToHost, s));
+    sync(ctx, "halo slots");
+    if (total != A) fail(GEO_ERR_CUDA, "halo slot count mismatch");
+    op->halo64.alloc(A);
+    op->halo32.alloc(A);
+    // slots of Dirichlet entries are never written (the node update ignores them)
+    GEO_CUDA(cudaMemsetAsync(op->halo64.p, 0, op->halo64.bytes(), s));
+    GEO_CUDA(cudaMemsetAsync(op->halo32.p, 0, op->halo32.bytes(), s));
+    op->halo_ok = true;
 }
 
 // Recomputes qdata, diagonal, char_diag and the Jacobi inverse from op->coef.
@@ -695,6 +818,8 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
                                                   op->fflags.p);
         check_launch(ctx, "k_patch_foreign");
         sync(ctx, "foreign segments");
+        op->n_app = pf[P];
+        if (dpn == 1 && op->n_app > 0) build_halo_slots(op.get(), acc);
     }
     // affine (straight-sided) elements use one metric per element
     DevBuf<int> aff(1);
@@ -720,11 +845,17 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
     });
     with_kernels(op.get(), [&](auto k64, auto k32) {
         int per_sm = 0;
-        GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, k_pcg_update<double, decltype(k64)::DPN, false>, kNodeBS, 0));
+        if (op->halo[0])
+            GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_update_halo<double, false>, kNodeBS, 0));
+        else
+            GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, k_pcg_update<double, decltype(k64)::DPN, false>, kNodeBS, 0));
         op->node_grid[0] = std::max(1, per_sm) * ctx->sm_count;
-        GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, k_pcg_update<float, decltype(k32)::DPN, true>, kNodeBS, 0));
+        if (op->halo[1])
+            GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_update_halo<float, true>, kNodeBS, 0));
+        else
+            GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, k_pcg_update<float, decltype(k32)::DPN, true>, kNodeBS, 0));
         op->node_grid[1] = std::max(1, per_sm) * ctx->sm_count;
     });
     op->bvec.alloc(op->ndof);
@@ -786,13 +917,23 @@ void lift_new(geo_op* op, const double* f_orig_dev, double* fbc_new) {
     sync(op->ctx, "lift");
 }
 
+// The node update of the PCG loop: the halo-mode kernel when the patch kernel runs
+// in halo mode.
+template <class K, class T, bool MIXED>
+void launch_update(const geo_op* op, cudaStream_t s, const NodeArgs<T>& na) {
+    constexpr int slot = std::is_same<T, double>::value ? 0 : 1;
+    const unsigned g = (unsigned)op->node_grid[slot];
+    if (K::DPN == 1 && op->halo[slot]) k_pcg_update_halo<T, MIXED><<<g, kNodeBS, 0, s>>>(na);
+    else k_pcg_update<T, K::DPN, MIXED><<<g, kNodeBS, 0, s>>>(na);
+}
+
 // Enqueues one PCG iteration (patch kernel in PCG mode + node update).
 template <class K, class T, bool MIXED>
 void enqueue_iteration(geo_op* op, cudaStream_t s, const PatchArgs<T>& pa, const NodeArgs<T>& na) {
     constexpr bool dbl = std::is_same<T, double>::value;
     const T* qd = dbl ? (const T*)op->qd64.p : (const T*)op->qd32.p;
     launch_patch<K, T, MODE_PCG>(op, dbl ? 0 : 1, s, qd, pa);
-    k_pcg_update<T, K::DPN, MIXED><<<(unsigned)op->node_grid[dbl ? 0 : 1], kNodeBS, 0, s>>>(na);
+    launch_update<K, T, MIXED>(op, s, na);
 }
 
 // Kernel arguments of the PCG loop over the operator's workspace (FP64 mode: r, q,
@@ -850,6 +991,14 @@ PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
         p32.pbuf0 = n32.pbuf0;
         p32.pbuf1 = n32.pbuf1;
         p32.y = n32.q;
+    }
+    if (op->halo[0]) {
+        n64.halo = p64.halo = op->halo64.p;
+        n64.hbase = op->hbase.p;
+    }
+    if (op->halo[1]) {
+        n32.halo = p32.halo = op->halo32.p;
+        n32.hbase = op->hbase.p;
     }
     auto al = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };
     n64.vec = al(n64.x) && al(n64.r) && al(n64.q) && al(n64.dinv) && al(n64.pbuf0) && al(n64.pbuf1);
@@ -983,15 +1132,14 @@ void time_iterations(geo_op* op, bool mixed, int iters, double* patch_ms, double
         }
     } guard{ev};
     for (auto& e : ev) GEO_CUDA(cudaEventCreate(&e));
-    const unsigned ng = (unsigned)op->node_grid[mixed ? 1 : 0];
     with_kernels(op, [&](auto k64, auto k32) {
         for (int i = 0; i < iters; ++i) {
             GEO_CUDA(cudaEventRecord(ev[2 * i], s));
             if (mixed) launch_patch<decltype(k32), float, MODE_PCG>(op, 1, s, op->qd32.p, la.p32);
             else launch_patch<decltype(k64), double, MODE_PCG>(op, 0, s, op->qd64.p, la.p64);
             GEO_CUDA(cudaEventRecord(ev[2 * i + 1], s));
-            if (mixed) k_pcg_update<float, decltype(k32)::DPN, true><<<ng, kNodeBS, 0, s>>>(la.n32);
-            else k_pcg_update<double, decltype(k64)::DPN, false><<<ng, kNodeBS, 0, s>>>(la.n64);
+            if (mixed) launch_update<decltype(k32), float, true>(op, s, la.n32);
+            else launch_update<decltype(k64), double, false>(op, s, la.n64);
         }
     });
     GEO_CUDA(cudaEventRecord(ev[2 * iters], s));

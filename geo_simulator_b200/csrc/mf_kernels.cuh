@@ -14,7 +14,11 @@
 //      (exact INT32 fixed point for FP32, see Scatter). Elements are ordered so
 //      a warp's 32 elements share no node, so these atomics do not collide;
 //   3. flush: a plain store for nodes no other patch touches, red.global.add
-//      for the shared ones.
+//      for the shared ones. In the PCG mode of one-DOF operators ("halo" mode)
+//      every own node is a plain store and every foreign node a plain store to
+//      its own slot of a halo array; the slots are numbered by owner node, so the
+//      node update adds a node's foreign contributions from consecutive slots in
+//      a fixed order. The PCG loop then issues no global atomics.
 // In PCG mode step 1 also forms the new search direction p = z + beta p_old
 // (z = D^-1 r) on the fly: the Jacobi scaling and the p-update ride on the
 // operator's gather. p is double-buffered by iteration parity.
@@ -64,6 +68,10 @@ struct PatchView {
     int max_for;
     int max_own;   // the largest own-node count of a patch
     int own_bulk;  // own-node slices by bulk copy (FP32 thermal PCG; the launch's shared memory holds them)
+    // halo mode (PCG, one DOF per node): the halo slot of every foreign entry, in
+    // the same per-patch segments as fids
+    const int32_t* fslot;
+    int halo;
 };
 
 // ------------------------------------------------------------------ shared-memory scatter
@@ -158,6 +166,7 @@ struct PatchArgs {
     PcgState* st;
     double* part;  // [gridDim.x][2]
     int* err;      // DEV_ERR_* bits (bounded waits)
+    T* halo;       // halo mode: foreign contributions by slot
 };
 
 // ------------------------------------------------------------------ bulk copy + mbarrier
@@ -227,13 +236,16 @@ struct PatchMeta {
     int pad0, pad1;
 };
 
-// per-buffer bytes of [meta | foreign ids | foreign flags]
+// per-buffer bytes of [meta | foreign ids | foreign flags | halo slots (halo mode)]
 __host__ __device__ inline uint32_t patch_aux_ids(int max_for) {
     return round16((uint32_t)((max_for + kForeignAlign - 1) / kForeignAlign * kForeignAlign) * 4u);
 }
-__host__ __device__ inline uint32_t patch_aux_bytes(int max_for) {
-    return (uint32_t)sizeof(PatchMeta) + patch_aux_ids(max_for) +
-           round16((uint32_t)((max_for + kForeignAlign - 1) / kForeignAlign * kForeignAlign));
+__host__ __device__ inline uint32_t patch_aux_flags(int max_for) {
+    return round16((uint32_t)((max_for + kForeignAlign - 1) / kForeignAlign * kForeignAlign));
+}
+__host__ __device__ inline uint32_t patch_aux_bytes(int max_for, int halo) {
+    return (uint32_t)sizeof(PatchMeta) + patch_aux_ids(max_for) + patch_aux_flags(max_for) +
+           (halo ? patch_aux_ids(max_for) : 0u);
 }
 
 // Own-node slices (PCG mode): D^-1, r and p_old over the patch's own DOF range
@@ -262,8 +274,8 @@ __host__ __device__ constexpr size_t patch_smem_fixed() {
     return 32 + (size_t)NBUF * (patch_bytes_lc<K, T>() + patch_bytes_qd<K, T>());
 }
 template <class K, class T, int NBUF>
-__host__ __device__ inline size_t patch_smem_tables(int max_for) {
-    return patch_smem_fixed<K, T, NBUF>() + (size_t)NBUF * patch_aux_bytes(max_for);
+__host__ __device__ inline size_t patch_smem_tables(int max_for, int halo) {
+    return patch_smem_fixed<K, T, NBUF>() + (size_t)NBUF * patch_aux_bytes(max_for, halo);
 }
 
 template <class K, class T, int MODE, int NBUF>
@@ -278,8 +290,10 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     using SC = Scatter<T>;
     const int M = pv.max_local * DPN;  // DOF slots of the patch-local table
     unsigned char* abuf = smem + patch_smem_fixed<K, T, NBUF>();  // NBUF x (meta | ids | flags)
-    const uint32_t AUX = patch_aux_bytes(pv.max_for), AIDS = patch_aux_ids(pv.max_for);
-    T* xs = reinterpret_cast<T*>(smem + patch_smem_tables<K, T, NBUF>(pv.max_for));
+    const bool HALO = MODE == MODE_PCG && DPN == 1 && pv.halo != 0;
+    const uint32_t AUX = patch_aux_bytes(pv.max_for, HALO), AIDS = patch_aux_ids(pv.max_for);
+    const uint32_t AFL = patch_aux_flags(pv.max_for);
+    T* xs = reinterpret_cast<T*>(smem + patch_smem_tables<K, T, NBUF>(pv.max_for, HALO));
     int* ys = reinterpret_cast<int*>(xs + M);  // fixed-point accumulators, SC::kWords x M words
     // FP32 scatter: per component, min and max of x over the patch as order keys, by patch parity
     __shared__ unsigned s_lo[2][DPN], s_hi[2][DPN];
@@ -323,12 +337,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         *reinterpret_cast<PatchMeta*>(ab) = m;  // published by the arrive below
         const uint32_t ib = round16((uint32_t)m.nfor * 4u), fb = round16((uint32_t)m.nfor);
         unsigned char* dst = ebuf + (size_t)b * (LCB + QDB);
-        mbar_expect_tx(&bar[b], LCB + QDB + ib + fb);
+        mbar_expect_tx(&bar[b], LCB + QDB + ib + fb + (HALO ? ib : 0u));
         bulk_g2s(dst, pv.lc + (size_t)patch * 5 * kPatchElems, LCB, &bar[b]);
         bulk_g2s(dst + LCB, qd_all + (size_t)patch * K::NQD * kPatchElems, QDB, &bar[b]);
         if (ib) {
             bulk_g2s(ab + sizeof(PatchMeta), pv.fids + m.fa, ib, &bar[b]);
             bulk_g2s(ab + sizeof(PatchMeta) + AIDS, pv.fflags + m.fa, fb, &bar[b]);
+            if (HALO) bulk_g2s(ab + sizeof(PatchMeta) + AIDS + AFL, pv.fslot + m.fa, ib, &bar[b]);
         }
     };
     // thread 0: D^-1, r, p_old and flags of the patch's own nodes (single buffer, bar[2])
@@ -388,6 +403,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         const PatchMeta pm = *reinterpret_cast<const PatchMeta*>(ab);
         const int* __restrict__ sfor = reinterpret_cast<const int*>(ab + sizeof(PatchMeta));
         const uint8_t* __restrict__ sffl = ab + sizeof(PatchMeta) + AIDS;
+        const int* __restrict__ sfsl = reinterpret_cast<const int*>(ab + sizeof(PatchMeta) + AIDS + AFL);
         const int n_el = pm.n_el, o0 = pm.o0, nown = pm.nown, nloc = nown + pm.nfor;
         const float pbound = pm.bound;
         float xlo[DPN], xhi[DPN];
@@ -530,8 +546,15 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         __syncthreads();
         // 3. flush (node ids: the own range, then the foreign list still in the aux buffer)
         for (int u = threadIdx.x; u < nloc; u += blockDim.x) {
-            const int node = u < nown ? o0 + u : sfor[u - nown];
             const uint8_t fl = sfl[u];
+            if (HALO) {  // one DOF per node: own nodes stored, foreign ones to their halo slots
+                if (fl & 1) continue;
+                const T v = SC::get(ys, M, u) * invS;
+                if (u < nown) a.y[o0 + u] = v;
+                else a.halo[sfsl[u - nown]] = v;
+                continue;
+            }
+            const int node = u < nown ? o0 + u : sfor[u - nown];
             const bool plain = u < nown && !(fl & kFlagShared);
 #pragma unroll
             for (int c = 0; c < DPN; ++c) {
@@ -588,6 +611,11 @@ struct NodeArgs {
     double* w64;
     const double* b;
     int vec;  // x, r, q, dinv, pbuf0 and pbuf1 are 16-byte aligned: k_pcg_update uses 16-byte loads
+    // halo mode (one DOF per node): foreign contributions by slot; node i's slots
+    // follow those of nodes < i, hbase[c] = slots of nodes < 32 c, flag bits 3-6 =
+    // the node's slot count
+    const T* halo;
+    const int32_t* hbase;
 };
 
 // 16-byte vector of T
@@ -607,6 +635,183 @@ struct Vec16<double> {
 // x += alpha p, r -= alpha q, z = D^-1 r; r.r and r.z; stopping / refresh decision.
 // With aligned vectors (a.vec) every thread streams 16-byte loads of p, q, x, r
 // and D^-1, kUnroll vectors in flight, and a scalar loop covers the tail.
+// r.r and r.z partials of the node update; the last block sums them, tests
+// convergence (FP64) or the refresh criteria (mixed) and sets beta.
+template <class T, bool MIXED>
+__device__ __forceinline__ void pcg_update_finish(const NodeArgs<T>& a, T acc_rr, T acc_rz) {
+    PcgState* st = a.st;
+    double v[2] = {(double)acc_rr, (double)acc_rz};
+    store_partial<2>(a.part, v);
+    if (last_block(&st->ticket[TICKET_UPDATE])) {
+        double t[2];
+        grid_total<2>(a.part, gridDim.x, t);
+        if (threadIdx.x == 0) {
+            st->ticket[TICKET_UPDATE] = 0;
+            const double rn = sqrt(t[0]);
+            if (!MIXED) {
+                st->res = rn;
+                if (rn < st->tol * st->bnorm || rn < st->abs_tol) {  // iterative.rs:95
+                    st->flags |= ST_DONE | ST_CONVERGED;
+                    return;
+                }
+            }
+            st->beta = t[1] / st->rz;
+            st->rz_old = st->rz;
+            st->rz = t[1];
+            st->it += 1;
+            if (MIXED) {
+                st->rmax = fmax(st->rmax, rn);
+                const double est = rn * st->s_scale;
+                if (est < st->tol * st->bnorm || est < st->abs_tol || rn < st->delta * st->rmax ||
+                    st->it >= st->max_it)
+                    st->flags |= ST_REFRESH;
+            } else if (st->it >= st->max_it) {
+                st->flags |= ST_DONE;
+            }
+        }
+    }
+}
+
+// k_pcg_update_halo: one 16-byte vector per array in flight per thread, four
+// resident blocks (64 registers). The halo loads wait on the slot scan, so warps
+// hide that latency better than deeper unrolling: at 128^3 (FP32) 0.095 ms
+// against 0.107 ms (two vectors) and 0.20 ms (four, one block per SM).
+constexpr int kHaloUnroll = 1;
+constexpr int kHaloMinBlocks = 4;
+constexpr int kHaloShift = 3;  // flag bits 3-6: halo slots of the node (halo mode)
+
+// Sum of node j's halo slots, starting at slot s (fixed order: slot order).
+template <class T>
+__device__ __forceinline__ T halo_sum(const T* __restrict__ halo, int64_t s, int cnt) {
+    T h = T(0);
+    for (int i = 0; i < cnt; ++i) h += halo[s + i];
+    return h;
+}
+
+// Node update of a one-DOF operator in halo mode: as the loops of k_pcg_update,
+// with q_j = (own-patch sum, stored by the patch kernel) + (node j's halo slots).
+// Lane l of a warp takes vector iv (V nodes); the warp's 32 vectors are 32 V
+// consecutive nodes starting at a multiple of 32, so its first slot is
+// hbase[first / 32] and each lane's first slot follows from a warp scan of the
+// lanes' slot counts. Loop conditions are warp-uniform (lanes past the end load
+// nothing and count 0 slots).
+template <class T, int kU>
+__device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T cd, const T* __restrict__ p,
+                                                T& acc_rr, T& acc_rz) {
+    using VT = typename Vec16<T>::type;
+    constexpr int V = Vec16<T>::N;
+    const uint8_t* __restrict__ flags = a.flags;
+    const T* __restrict__ dinv = a.dinv;
+    const T* __restrict__ halo = a.halo;
+    T* __restrict__ x = a.x;
+    T* __restrict__ r = a.r;
+    const T* __restrict__ q = a.q;
+    const int lane = threadIdx.x & 31;
+    const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    auto entry = [&](T pj, T qj, T xj, T rj, T dj, uint8_t f, T& xo, T& ro) {
+        const T qq = (f & 1) ? cd * pj : qj;
+        xo = xj + alpha * pj;
+        ro = rj - alpha * qq;
+        acc_rr += ro * ro;
+        acc_rz += ro * (ro * dj);
+    };
+    // first slot of this lane's V nodes; every lane of the warp calls it
+    auto lane_slot = [&](int64_t iv, int tot) {
+        int incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int64_t first = __shfl_sync(0xffffffffu, iv, 0) * V;
+        return (int64_t)a.hbase[first / 32] + (incl - tot);
+    };
+    const int64_t nv = a.vec ? n / V : 0;
+    int64_t iv = tid;
+    for (; iv - lane + 31 + (kU - 1) * nth < nv; iv += kU * nth) {  // all lanes, all u in range
+        VT pv[kU], qv[kU], xv[kU], rv[kU], dv[kU];
+        uint8_t fl[kU][V];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int64_t k = iv + u * nth;
+            pv[u] = reinterpret_cast<const VT*>(p)[k];
+            qv[u] = reinterpret_cast<const VT*>(q)[k];
+            xv[u] = reinterpret_cast<const VT*>(x)[k];
+            rv[u] = reinterpret_cast<const VT*>(r)[k];
+            dv[u] = reinterpret_cast<const VT*>(dinv)[k];
+#pragma unroll
+            for (int e = 0; e < V; ++e) fl[u][e] = flags[k * V + e];
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int64_t k = iv + u * nth;
+            int cnt[V], tot = 0;
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+                cnt[e] = (fl[u][e] >> kHaloShift) & 15;
+                tot += cnt[e];
+            }
+            int64_t sl = lane_slot(k, tot);
+            const T* pe = reinterpret_cast<const T*>(&pv[u]);
+            const T* qe = reinterpret_cast<const T*>(&qv[u]);
+            const T* xe = reinterpret_cast<const T*>(&xv[u]);
+            const T* re = reinterpret_cast<const T*>(&rv[u]);
+            const T* de = reinterpret_cast<const T*>(&dv[u]);
+            VT xo, ro;
+            T* xoe = reinterpret_cast<T*>(&xo);
+            T* roe = reinterpret_cast<T*>(&ro);
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+                const T qj = qe[e] + halo_sum(halo, sl, cnt[e]);
+                sl += cnt[e];
+                entry(pe[e], qj, xe[e], re[e], de[e], fl[u][e], xoe[e], roe[e]);
+            }
+            reinterpret_cast<VT*>(x)[k] = xo;
+            reinterpret_cast<VT*>(r)[k] = ro;
+        }
+    }
+    for (; iv - lane < nv; iv += nth) {  // warp-uniform: some lanes may be past nv
+        const bool in = iv < nv;
+        uint8_t fl[V];
+        int cnt[V], tot = 0;
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            fl[e] = in ? flags[iv * V + e] : (uint8_t)0;
+            cnt[e] = (fl[e] >> kHaloShift) & 15;
+            tot += cnt[e];
+        }
+        int64_t sl = lane_slot(iv, tot);
+        if (in) {
+            const VT pv = reinterpret_cast<const VT*>(p)[iv], qv = reinterpret_cast<const VT*>(q)[iv];
+            const VT xv = reinterpret_cast<const VT*>(x)[iv], rv = reinterpret_cast<const VT*>(r)[iv];
+            const VT dv = reinterpret_cast<const VT*>(dinv)[iv];
+            VT xo, ro;
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+                const T qj = reinterpret_cast<const T*>(&qv)[e] + halo_sum(halo, sl, cnt[e]);
+                sl += cnt[e];
+                entry(reinterpret_cast<const T*>(&pv)[e], qj, reinterpret_cast<const T*>(&xv)[e],
+                      reinterpret_cast<const T*>(&rv)[e], reinterpret_cast<const T*>(&dv)[e], fl[e],
+                      reinterpret_cast<T*>(&xo)[e], reinterpret_cast<T*>(&ro)[e]);
+            }
+            reinterpret_cast<VT*>(x)[iv] = xo;
+            reinterpret_cast<VT*>(r)[iv] = ro;
+        }
+    }
+    // the last n mod V nodes (all nodes when the vectors are not 16-byte aligned):
+    // the slot base from the 32-node chunk start
+    for (int64_t j = nv * V + tid; j < n; j += nth) {
+        const uint8_t f = flags[j];
+        int64_t sl = a.hbase[j / 32];
+        for (int64_t i = j & ~(int64_t)31; i < j; ++i) sl += (flags[i] >> kHaloShift) & 15;
+        T xo, ro;
+        entry(p[j], q[j] + halo_sum(halo, sl, (f >> kHaloShift) & 15), x[j], r[j], dinv[j], f, xo, ro);
+        x[j] = xo;
+        r[j] = ro;
+    }
+}
+
 template <class T, int DPN, bool MIXED>
 __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
     PcgState* st = a.st;
@@ -684,36 +889,18 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
         x[j] = xo;
         r[j] = ro;
     }
-    double v[2] = {(double)acc_rr, (double)acc_rz};
-    store_partial<2>(a.part, v);
-    if (last_block(&st->ticket[TICKET_UPDATE])) {
-        double t[2];
-        grid_total<2>(a.part, gridDim.x, t);
-        if (threadIdx.x == 0) {
-            st->ticket[TICKET_UPDATE] = 0;
-            const double rn = sqrt(t[0]);
-            if (!MIXED) {
-                st->res = rn;
-                if (rn < st->tol * st->bnorm || rn < st->abs_tol) {  // iterative.rs:95
-                    st->flags |= ST_DONE | ST_CONVERGED;
-                    return;
-                }
-            }
-            st->beta = t[1] / st->rz;
-            st->rz_old = st->rz;
-            st->rz = t[1];
-            st->it += 1;
-            if (MIXED) {
-                st->rmax = fmax(st->rmax, rn);
-                const double est = rn * st->s_scale;
-                if (est < st->tol * st->bnorm || est < st->abs_tol || rn < st->delta * st->rmax ||
-                    st->it >= st->max_it)
-                    st->flags |= ST_REFRESH;
-            } else if (st->it >= st->max_it) {
-                st->flags |= ST_DONE;
-            }
-        }
-    }
+    pcg_update_finish<T, MIXED>(a, acc_rr, acc_rz);
+}
+
+// Node update of a one-DOF operator's PCG in halo mode (see pcg_update_halo).
+template <class T, bool MIXED>
+__global__ void __launch_bounds__(kNodeBS, kHaloMinBlocks) k_pcg_update_halo(NodeArgs<T> a) {
+    PcgState* st = a.st;
+    if (st->flags & (ST_DONE | ST_REFRESH)) return;
+    const T* __restrict__ p = (st->it & 1) ? a.pbuf0 : a.pbuf1;
+    T acc_rr = T(0), acc_rz = T(0);
+    pcg_update_halo<T, kHaloUnroll>(a, (T)st->alpha, (T)st->cd, p, acc_rr, acc_rz);
+    pcg_update_finish<T, MIXED>(a, acc_rr, acc_rz);
 }
 
 // FP64 mode start: x = 0, r = b, p_old = 0, q = 0; ||b||, r.z.

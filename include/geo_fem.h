@@ -93,6 +93,12 @@ int geo_ctx_create(int device, geo_ctx** out);
 int geo_ctx_destroy(geo_ctx* ctx);
 const char* geo_last_error(const geo_ctx* ctx);
 const char* geo_version(void);
+/* No counterpart in the reference. Device memory of destroyed objects and finished
+ * calls is kept by the library and reused by later calls of the same sizes (freed
+ * only after the device has finished the work queued before). This returns the
+ * kept memory of every device to the driver; geo_ctx_destroy does so for its
+ * device, and an allocation that runs out of memory does so before retrying. */
+int geo_release_cached_memory(void);
 int geo_sm_count(const geo_ctx* ctx, int* sm_count);
 /* The context's CUDA stream (cudaStream_t), so callers can order or time their
  * own work against the library's launches. */
