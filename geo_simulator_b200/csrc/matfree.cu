@@ -524,7 +524,7 @@ PatchView view(const geo_op* op) {
 
 // dynamic shared memory of the patch kernel: barriers, element-data buffers, node tables
 template <class K, class T>
-size_t smem_bytes(const geo_op* op, int nbuf, bool own, bool halo = false) {
+size_t smem_bytes(const geo_op* op, int nbuf, bool own, int halo = 0) {
     // xs (T), fixed-point accumulators (Scatter<T>::kWords INT32 words), flags, and for
     // FP32 thermal PCG the own-node slices
     const size_t tables = (size_t)op->max_local * K::DPN * (sizeof(T) + 4 * Scatter<T>::kWords) +
@@ -555,6 +555,8 @@ int setup_patch_nbuf(size_t attr_bytes, size_t plain, size_t own, int& per_sm_pl
     GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_LIFT, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)attr_bytes));
     GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_PCG, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)attr_bytes));
+    GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_PCG, NBUF, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)attr_bytes));
     per_sm_plain = 0;
     GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_plain, k_patch<K, T, MODE_PCG, NBUF>, kPatchBS,
@@ -590,13 +592,14 @@ int setup_patch_kernels(geo_op* op, int slot) {
     op->patch_smem[slot] = op->own_bulk[slot] ? own : plain;
     if (per_sm < 1) fail(GEO_ERR_UNSUPPORTED, "patch kernel does not fit on an SM");
     per_sm = std::max(per_sm, per_sm_own);
-    // halo mode (one DOF per node) when its slot lists cost no resident block
+    // halo mode for one-DOF operators: slots in the bulk copy when that costs no
+    // resident block, else read by the flush from global memory
     op->halo[slot] = 0;
     if (K::DPN == 1 && op->halo_ok) {
-        const size_t hs = smem_bytes<K, T>(op, nbuf, op->own_bulk[slot] != 0, true);
+        op->halo[slot] = 2;
+        const size_t hs = smem_bytes<K, T>(op, nbuf, op->own_bulk[slot] != 0, 1);
         int per_sm_halo = 0;
-        if (hs <= kSmemLimit) {
-            // raises the limit of every mode's kernel (all launch with patch_smem[slot])
+        if (hs <= kSmemLimit) {  // raises the limit of every mode (all launch with patch_smem[slot])
             const size_t attr = std::max(hs, std::max(plain, own));
             if (nbuf == 2) setup_patch_nbuf<K, T, 2>(attr, hs, 0, per_sm_halo);
             else setup_patch_nbuf<K, T, 1>(attr, hs, 0, per_sm_halo);
@@ -616,10 +619,14 @@ void launch_patch(const geo_op* op, int slot, cudaStream_t s, const T* qd, const
     v.own_bulk = op->own_bulk[slot];
     v.halo = MODE == MODE_PCG ? op->halo[slot] : 0;
     const size_t smem = op->patch_smem[slot];
-    if (op->nbuf[slot] == 2)
-        k_patch<K, T, MODE, 2><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
-    else
-        k_patch<K, T, MODE, 1><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
+    const bool hg = MODE == MODE_PCG && v.halo == 2;
+    if (op->nbuf[slot] == 2) {
+        if (hg) k_patch<K, T, MODE, 2, 1><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
+        else k_patch<K, T, MODE, 2><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
+    } else {
+        if (hg) k_patch<K, T, MODE, 1, 1><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
+        else k_patch<K, T, MODE, 1><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
+    }
 }
 
 // Halo slots of a one-DOF operator (see k_halo_count): fslot in the fids

@@ -69,7 +69,9 @@ struct PatchView {
     int max_own;   // the largest own-node count of a patch
     int own_bulk;  // own-node slices by bulk copy (FP32 thermal PCG; the launch's shared memory holds them)
     // halo mode (PCG, one DOF per node): the halo slot of every foreign entry, in
-    // the same per-patch segments as fids
+    // the same per-patch segments as fids. halo: 0 off; 1 the slots ride in the
+    // patch's bulk copy; 2 the flush reads them from global memory (coalesced), for
+    // launches where the shared-memory copy would cost a resident block
     const int32_t* fslot;
     int halo;
 };
@@ -236,7 +238,7 @@ struct PatchMeta {
     int pad0, pad1;
 };
 
-// per-buffer bytes of [meta | foreign ids | foreign flags | halo slots (halo mode)]
+// per-buffer bytes of [meta | foreign ids | foreign flags | halo slots (halo == 1)]
 __host__ __device__ inline uint32_t patch_aux_ids(int max_for) {
     return round16((uint32_t)((max_for + kForeignAlign - 1) / kForeignAlign * kForeignAlign) * 4u);
 }
@@ -245,7 +247,7 @@ __host__ __device__ inline uint32_t patch_aux_flags(int max_for) {
 }
 __host__ __device__ inline uint32_t patch_aux_bytes(int max_for, int halo) {
     return (uint32_t)sizeof(PatchMeta) + patch_aux_ids(max_for) + patch_aux_flags(max_for) +
-           (halo ? patch_aux_ids(max_for) : 0u);
+           (halo == 1 ? patch_aux_ids(max_for) : 0u);
 }
 
 // Own-node slices (PCG mode): D^-1, r and p_old over the patch's own DOF range
@@ -278,7 +280,9 @@ __host__ __device__ inline size_t patch_smem_tables(int max_for, int halo) {
     return patch_smem_fixed<K, T, NBUF>() + (size_t)NBUF * patch_aux_bytes(max_for, halo);
 }
 
-template <class K, class T, int MODE, int NBUF>
+// HG = 1: the halo-mode variant whose flush reads the halo slots from global
+// memory (PatchView::halo == 2); HG = 0 serves every other launch.
+template <class K, class T, int MODE, int NBUF, int HG = 0>
 __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __restrict__ qd_all, T cl, T cm,
                                                     PatchArgs<T> a) {
     constexpr int DPN = K::DPN;
@@ -290,10 +294,11 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     using SC = Scatter<T>;
     const int M = pv.max_local * DPN;  // DOF slots of the patch-local table
     unsigned char* abuf = smem + patch_smem_fixed<K, T, NBUF>();  // NBUF x (meta | ids | flags)
-    const bool HALO = MODE == MODE_PCG && DPN == 1 && pv.halo != 0;
-    const uint32_t AUX = patch_aux_bytes(pv.max_for, HALO), AIDS = patch_aux_ids(pv.max_for);
+    const bool HALO = MODE == MODE_PCG && DPN == 1 && (HG != 0 || pv.halo != 0);
+    const int HMODE = !HALO ? 0 : (HG ? 2 : 1);  // 1: slots in shared memory, 2: from global
+    const uint32_t AUX = patch_aux_bytes(pv.max_for, HMODE), AIDS = patch_aux_ids(pv.max_for);
     const uint32_t AFL = patch_aux_flags(pv.max_for);
-    T* xs = reinterpret_cast<T*>(smem + patch_smem_tables<K, T, NBUF>(pv.max_for, HALO));
+    T* xs = reinterpret_cast<T*>(smem + patch_smem_tables<K, T, NBUF>(pv.max_for, HMODE));
     int* ys = reinterpret_cast<int*>(xs + M);  // fixed-point accumulators, SC::kWords x M words
     // FP32 scatter: per component, min and max of x over the patch as order keys, by patch parity
     __shared__ unsigned s_lo[2][DPN], s_hi[2][DPN];
@@ -337,13 +342,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         *reinterpret_cast<PatchMeta*>(ab) = m;  // published by the arrive below
         const uint32_t ib = round16((uint32_t)m.nfor * 4u), fb = round16((uint32_t)m.nfor);
         unsigned char* dst = ebuf + (size_t)b * (LCB + QDB);
-        mbar_expect_tx(&bar[b], LCB + QDB + ib + fb + (HALO ? ib : 0u));
+        mbar_expect_tx(&bar[b], LCB + QDB + ib + fb + (HMODE == 1 ? ib : 0u));
         bulk_g2s(dst, pv.lc + (size_t)patch * 5 * kPatchElems, LCB, &bar[b]);
         bulk_g2s(dst + LCB, qd_all + (size_t)patch * K::NQD * kPatchElems, QDB, &bar[b]);
         if (ib) {
             bulk_g2s(ab + sizeof(PatchMeta), pv.fids + m.fa, ib, &bar[b]);
             bulk_g2s(ab + sizeof(PatchMeta) + AIDS, pv.fflags + m.fa, fb, &bar[b]);
-            if (HALO) bulk_g2s(ab + sizeof(PatchMeta) + AIDS + AFL, pv.fslot + m.fa, ib, &bar[b]);
+            if (HMODE == 1) bulk_g2s(ab + sizeof(PatchMeta) + AIDS + AFL, pv.fslot + m.fa, ib, &bar[b]);
         }
     };
     // thread 0: D^-1, r, p_old and flags of the patch's own nodes (single buffer, bar[2])
@@ -551,7 +556,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                 if (fl & 1) continue;
                 const T v = SC::get(ys, M, u) * invS;
                 if (u < nown) a.y[o0 + u] = v;
-                else a.halo[sfsl[u - nown]] = v;
+                else a.halo[HG ? __ldg(pv.fslot + pm.fa + (u - nown)) : sfsl[u - nown]] = v;
                 continue;
             }
             const int node = u < nown ? o0 + u : sfor[u - nown];
