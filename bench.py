@@ -88,10 +88,9 @@ def solve_bytes(E, N, iters, nupd):
 
 
 # DRAM bytes (read + write) per element of one FP32 PCG-mode patch-kernel launch,
-# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the 96^3 cube
-# (5,308,416 elements: 424.7 MB per launch); the traffic scales with the element
-# count (the node/element ratio of the cube is 1.35 at both sizes).
-PATCH_PCG_F32_DRAM_BYTES_PER_ELEMENT = 80.0
+# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the bench's
+# 128^3 cube (12,582,912 elements: 1008.9 MB per launch).
+PATCH_PCG_F32_DRAM_BYTES_PER_ELEMENT = 80.18
 
 
 class ClockSampler:
@@ -297,10 +296,10 @@ def run_ours(args, ws, rank, local, pg):
         "gpu_launches": int(sum(s_.kernel_launches for s_ in st_mixed)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "k_patch<ThermalK<float,1>, float, MODE_PCG, 2>",
+                     "kernel": "k_patch<ThermalK<float,1>, float, MODE_PCG, 2, 0> (halo slots in shared memory)",
                      "algorithmic_bytes_per_launch": pbytes, "launch_s": patch_s,
                      "timing": f"CUDA events between launches, {kt_iters} PCG iterations after the timed region",
-                     "node_update": {"kernel": "k_pcg_update<float, 1, true>", "launch_s": update_s,
+                     "node_update": {"kernel": "k_pcg_update_halo<float, true>", "launch_s": update_s,
                                      "algorithmic_bytes_per_launch": ubytes,
                                      "achieved": ubytes / update_s / 1e9,
                                      "frac": ubytes / update_s / 1e9 / hbm},
