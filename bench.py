@@ -384,8 +384,9 @@ def adjoint_ratio(ctx, args):
     g = np.zeros_like(u)
     g[obs] = u[obs] - that[obs]
     reps = 5
-    op.forward(f, solver)
+    op.forward(f, solver)  # warm-up of each timed call
     op.vjp(g, u=u, solver=solver)
+    op.vjp(g, u=None, f=f, solver=solver)
     t0 = time.perf_counter()
     for _ in range(reps):
         u, sf = op.forward(f, solver)
