@@ -13,6 +13,7 @@
 // operator runs in halo mode instead: foreign contributions are stored to
 // per-entry slots and added by the node update in slot order, with no atomics.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <type_traits>
 
@@ -593,9 +594,13 @@ int setup_patch_kernels(geo_op* op, int slot) {
     if (per_sm < 1) fail(GEO_ERR_UNSUPPORTED, "patch kernel does not fit on an SM");
     per_sm = std::max(per_sm, per_sm_own);
     // halo mode for one-DOF operators: slots in the bulk copy when that costs no
-    // resident block, else read by the flush from global memory
+    // resident block, else read by the flush from global memory. GEO_PATCH_HALO
+    // (0: atomics, 1: slots in shared memory, 2: slots from global) forces a mode,
+    // so that tests cover all three on small meshes.
     op->halo[slot] = 0;
-    if (K::DPN == 1 && op->halo_ok) {
+    const char* force = std::getenv("GEO_PATCH_HALO");
+    const int forced = force && force[0] >= '0' && force[0] <= '2' && force[1] == 0 ? force[0] - '0' : -1;
+    if (K::DPN == 1 && op->halo_ok && forced != 0) {
         op->halo[slot] = 2;
         const size_t hs = smem_bytes<K, T>(op, nbuf, op->own_bulk[slot] != 0, 1);
         int per_sm_halo = 0;
@@ -604,9 +609,14 @@ int setup_patch_kernels(geo_op* op, int slot) {
             if (nbuf == 2) setup_patch_nbuf<K, T, 2>(attr, hs, 0, per_sm_halo);
             else setup_patch_nbuf<K, T, 1>(attr, hs, 0, per_sm_halo);
         }
-        if (per_sm_halo >= per_sm) {
+        if (per_sm_halo > 0 && (forced == 1 || (forced < 0 && per_sm_halo >= per_sm))) {
             op->halo[slot] = 1;
             op->patch_smem[slot] = hs;
+            if (forced == 1) per_sm = per_sm_halo;
+        }
+        if (forced == 2) {
+            op->halo[slot] = 2;
+            op->patch_smem[slot] = op->own_bulk[slot] ? own : plain;
         }
     }
     return per_sm * op->ctx->sm_count;

@@ -1,0 +1,47 @@
+"""The three ways the one-DOF PCG's patch kernel hands shared-node contributions
+to the node update: red.global.add (mode 0), halo slots carried in shared memory
+(1) and halo slots read from global memory (2). The operator set-up picks one
+by occupancy (2 only on large meshes); GEO_PATCH_HALO forces each here, and the
+solutions must agree with the oracle's CG and with each other, in FP64 and mixed
+precision. The node counts are not multiples of the node update's vector width,
+so its scalar tail runs too."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import thermal_problem
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [7, 12])
+def test_halo_modes_agree(orc, geo, n, monkeypatch):
+    xyz, conn, mask, vals = thermal_problem(n, orc)
+    rng = np.random.default_rng(n)
+    k_e = np.exp(np.log(3.0) + 0.5 * rng.normal(size=conn.shape[0]))
+    K = orc.assemble_thermal_stiffness(xyz, conn, k_e=k_e)
+    f = orc.assemble_thermal_load(xyz, conn, 1e-6)
+    Kbc, fbc = orc.apply_dirichlet_bcs(K, f, mask, vals)
+    ref, _ = orc.cg_solve(Kbc, fbc, max_iterations=20000, tolerance=1e-12)
+    mesh = geo.Mesh(xyz, conn)
+    dm = geo.DofManager(xyz.shape[0], 1)
+    idx = np.nonzero(mask)[0]
+    dm.set_dirichlet(idx, vals[idx])
+    fg = geo.Assembler.assemble_thermal_load(mesh, dm, 1e-6)
+    sols = {}
+    for mode in ("0", "1", "2"):
+        monkeypatch.setenv("GEO_PATCH_HALO", mode)
+        op = geo.ThermalOperator(mesh, dm, k_e)
+        for prec in ("fp64", "mixed"):
+            solver = geo.ConjugateGradient().with_tolerance(1e-10).with_max_iterations(20000).with_precision(prec)
+            u, st = op.forward(fg, solver)
+            assert st.converged, (mode, prec)
+            assert np.linalg.norm(u - ref) <= 1e-8 * np.linalg.norm(ref), (mode, prec)
+            sols[mode, prec] = (u, st.iterations)
+        del op
+    for prec in ("fp64", "mixed"):
+        u0, it0 = sols["0", prec]
+        for mode in ("1", "2"):
+            u, it = sols[mode, prec]
+            assert np.linalg.norm(u - u0) <= 1e-9 * np.linalg.norm(u0)
+            assert abs(it - it0) <= 3
