@@ -20,8 +20,11 @@ namespace geo {
 namespace {
 
 constexpr int kKBS = 256;
-constexpr int kKVec = 8;     // lanes per CSR row
-constexpr int kKUnroll = 4;  // row entries in flight per lane
+// SpMV row shape (lanes per CSR row, row entries in flight per lane): GMRES takes
+// the CG drop-in's four lanes x eight entries; BiCGSTAB, with two SpMVs and more
+// live vectors, keeps eight x four, which fits its 64 registers without spills.
+constexpr int kGmresVec = 4, kGmresUnroll = 8;
+constexpr int kBicgVec = 8, kBicgUnroll = 4;
 constexpr int kMaxRestart = 64;
 
 struct KrylovArgs {
@@ -45,6 +48,7 @@ struct KrylovArgs {
 };
 
 // (A x)_row for the sub-warp of kKVec lanes owning `row` (valid in lane sub == 0)
+template <int kKVec, int kKUnroll>
 __device__ __forceinline__ double csr_row(const KrylovArgs& a, int64_t row, int sub, const double* x) {
     double s = 0.0;
     if (row < a.n) {
@@ -104,6 +108,7 @@ __device__ __forceinline__ bool reduce(const KrylovArgs& a, int& turn, double (&
 
 // ------------------------------------------------------------------ BiCGSTAB (iterative.rs:177-278)
 __global__ void __launch_bounds__(kKBS, 4) k_bicgstab(KrylovArgs a) {
+    constexpr int kKVec = kBicgVec;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t nth = (int64_t)gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31, sub = lane % kKVec;
@@ -160,7 +165,7 @@ __global__ void __launch_bounds__(kKBS, 4) k_bicgstab(KrylovArgs a) {
             double q[1] = {0.0}, o[1];
             for (int64_t rbase = warp * rows_per_warp; rbase < n; rbase += nwarps * rows_per_warp) {
                 const int64_t row = rbase + lane / kKVec;
-                const double sv = csr_row(a, row, sub, ph);
+                const double sv = csr_row<kBicgVec, kBicgUnroll>(a, row, sub, ph);
                 if (row < n && sub == 0) {
                     v[row] = sv;
                     q[0] += rh[row] * sv;
@@ -197,7 +202,7 @@ __global__ void __launch_bounds__(kKBS, 4) k_bicgstab(KrylovArgs a) {
             double q[2] = {0.0, 0.0}, o[2];
             for (int64_t rbase = warp * rows_per_warp; rbase < n; rbase += nwarps * rows_per_warp) {
                 const int64_t row = rbase + lane / kKVec;
-                const double tv = csr_row(a, row, sub, sh);
+                const double tv = csr_row<kBicgVec, kBicgUnroll>(a, row, sub, sh);
                 if (row < n && sub == 0) {
                     t[row] = tv;
                     q[0] += tv * tv;
@@ -257,6 +262,7 @@ __device__ __forceinline__ void givens(double a, double b, double& c, double& s,
 }
 
 __global__ void __launch_bounds__(kKBS, 4) k_gmres(KrylovArgs a) {
+    constexpr int kKVec = kGmresVec;
     extern __shared__ double sm[];
     const int m = a.restart;
     double* H = sm;                    // (m + 1) x m, H[i * m + j]
@@ -298,7 +304,7 @@ __global__ void __launch_bounds__(kKBS, 4) k_gmres(KrylovArgs a) {
             double q[1] = {0.0}, o[1];
             for (int64_t rbase = warp * rows_per_warp; rbase < n; rbase += nwarps * rows_per_warp) {
                 const int64_t row = rbase + lane / kKVec;
-                const double ax = csr_row(a, row, sub, a.x);
+                const double ax = csr_row<kGmresVec, kGmresUnroll>(a, row, sub, a.x);
                 if (row < n && sub == 0) {
                     const double ri = a.b[row] - ax;
                     r[row] = ri;
@@ -331,7 +337,7 @@ __global__ void __launch_bounds__(kKBS, 4) k_gmres(KrylovArgs a) {
                 const double* v0 = Vj(0);
                 for (int64_t rbase = warp * rows_per_warp; rbase < n; rbase += nwarps * rows_per_warp) {
                     const int64_t row = rbase + lane / kKVec;
-                    const double wv = csr_row(a, row, sub, z);
+                    const double wv = csr_row<kGmresVec, kGmresUnroll>(a, row, sub, z);
                     if (row < n && sub == 0) {
                         w[row] = wv;
                         q[0] += v0[row] * wv;

@@ -4,6 +4,7 @@
         [--precision mixed|fp64] [--physics thermal|elasticity]
     python -m geo_simulator_b200.kernel_timing --meshgen --size 128
     python -m geo_simulator_b200.kernel_timing --vtu --size 128 [--vtu-file PATH]
+    python -m geo_simulator_b200.kernel_timing --csr --size 64 [--reps 2]
 
 Builds the n^3-hex ImprovedMeshGenerator cube (1000 x 1000 x 600, ln k_e ~
 N(ln 3, 0.5^2) from seed 1001, T = 1280 at z = 0 and 0 at z = 600, Q = 1e-6;
@@ -17,6 +18,11 @@ timed ones.
 With --meshgen it instead builds the same cube once on the device
 (geo_mesh_generate_cube: one launch each of k_cube_vertices, k_cube_midpoints
 and k_cube_conn) and prints its sizes and the mesh's algorithmic bytes.
+
+With --csr it assembles K_bc of the cube (k = 3) on the device and runs the FP64
+CSR Jacobi-PCG drop-in (geo_cg_solve, one persistent k_csr_pcg launch per solve)
+to rel-res 1e-8, timed with CUDA events, and prints the iteration count and the
+CSR bytes streamed per iteration.
 
 With --vtu it builds that device mesh, attaches a seeded temperature field
 (N(600, 300^2) per node, seed 9) and renders the VTU text into a device buffer
@@ -137,6 +143,35 @@ def build(size, physics):
     return mesh, op, op.lift_rhs(f)
 
 
+def csr_timing(n, reps):
+    """geo_cg_solve on the assembled n^3 thermal K_bc: (JSON-ready dict)."""
+    import torch
+
+    import geo_simulator_b200 as geo
+    from bench import Q, thermal_inputs
+    ctx = geo.Context.default()
+    mesh, _, mask, vals = thermal_inputs(n)
+    dm = geo.DofManager(mesh.num_nodes(), 1)
+    idx = np.nonzero(mask)[0]
+    dm.set_dirichlet(idx, vals[idx])
+    f = geo.Assembler.assemble_thermal_load(mesh, dm, Q, ctx)
+    fd = torch.from_numpy(f).to(torch.device("cuda", torch.cuda.current_device()))
+    Kb, fb = geo.Assembler.apply_dirichlet_bcs(geo.Assembler.assemble_thermal_stiffness_parallel(mesh, dm, 3.0, ctx),
+                                               fd, dm, ctx)
+    cg = geo.ConjugateGradient().with_tolerance(1e-8).with_max_iterations(20000)
+    times, its = [], 0
+    for _ in range(reps + 1):
+        _, st = cg.solve(Kb, fb)
+        times.append(st.solve_time)
+        its = st.iterations
+    t = min(times[1:]) if reps > 0 else times[0]
+    nnz, rows = Kb.nnz(), Kb.rows()
+    per_it = nnz * 12 + rows * 8 * 10  # CSR values + indices, and the vector streams of one iteration
+    return {"size": n, "rows": rows, "nnz": nnz, "iterations": its, "solve_s": t,
+            "ms_per_iteration": t / max(1, its) * 1e3, "bytes_per_iteration": per_it,
+            "gbs": per_it * its / t / 1e9}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--size", type=int, default=96)
@@ -146,10 +181,15 @@ def main():
     ap.add_argument("--meshgen", action="store_true")
     ap.add_argument("--vtu", action="store_true")
     ap.add_argument("--vtu-file", default=None)
+    ap.add_argument("--csr", action="store_true")
+    ap.add_argument("--reps", type=int, default=2)
     args = ap.parse_args()
     from geo_simulator_b200 import _native as N
     if args.vtu:
         print(json.dumps(vtu_timing(args.size, args.vtu_file)))
+        return
+    if args.csr:
+        print(json.dumps(csr_timing(args.size, args.reps)))
         return
     if args.meshgen:
         import geo_simulator_b200 as geo
