@@ -9,7 +9,7 @@
 // elements from the per-element qdata, accumulates into shared memory, and the
 // patch flushes its nodes: plain stores for nodes no other patch touches,
 // red.global.add for the shared ones (so the matrix-free apply is not
-// bit-reproducible in the last bit; the assembled path is). The PCG of a one-DOF
+// bit-reproducible in the last bit; the assembled path is). The PCG of the
 // operator runs in halo mode instead: foreign contributions are stored to
 // per-entry slots and added by the node update in slot order, with no atomics.
 #include <algorithm>
@@ -183,7 +183,7 @@ __global__ void k_patch_foreign(const int32_t* __restrict__ pf, const int32_t* _
     }
 }
 
-// Halo slots of a one-DOF operator's PCG: every foreign entry a (patch p, its
+// Halo slots of the PCG (thermal and elasticity): every foreign entry a (patch p, its
 // k-th foreign node n, a = pf[p] + k) gets a slot. Slots are ordered by node n,
 // then by entry (a stable sort of the entries by node), so node n's slots are
 // consecutive and follow those of the nodes before it.
@@ -445,7 +445,7 @@ struct geo_op {
     geo::DevBuf<uint8_t> fflags;
     int max_for = 0;
     int max_own = 0;  // largest own-node count of a patch
-    // halo mode of the PCG (one DOF per node): slot of every foreign entry (fids
+    // halo mode of the PCG: slot of every foreign entry (fids
     // segments), slots before each 32-node chunk, and the slot arrays
     geo::DevBuf<int32_t> fslot, hbase;
     geo::DevBuf<double> halo64;
@@ -593,14 +593,14 @@ int setup_patch_kernels(geo_op* op, int slot) {
     op->patch_smem[slot] = op->own_bulk[slot] ? own : plain;
     if (per_sm < 1) fail(GEO_ERR_UNSUPPORTED, "patch kernel does not fit on an SM");
     per_sm = std::max(per_sm, per_sm_own);
-    // halo mode for one-DOF operators: slots in the bulk copy when that costs no
+    // halo mode: slots in the bulk copy when that costs no
     // resident block, else read by the flush from global memory. GEO_PATCH_HALO
     // (0: atomics, 1: slots in shared memory, 2: slots from global) forces a mode,
     // so that tests cover all three on small meshes.
     op->halo[slot] = 0;
     const char* force = std::getenv("GEO_PATCH_HALO");
     const int forced = force && force[0] >= '0' && force[0] <= '2' && force[1] == 0 ? force[0] - '0' : -1;
-    if (K::DPN == 1 && op->halo_ok && forced != 0) {
+    if ((K::DPN == 1 || K::DPN == 3) && op->halo_ok && forced != 0) {
         op->halo[slot] = 2;
         const size_t hs = smem_bytes<K, T>(op, nbuf, op->own_bulk[slot] != 0, 1);
         int per_sm_halo = 0;
@@ -639,7 +639,7 @@ void launch_patch(const geo_op* op, int slot, cudaStream_t s, const T* qd, const
     }
 }
 
-// Halo slots of a one-DOF operator (see k_halo_count): fslot in the fids
+// Halo slots (see k_halo_count): fslot in the fids
 // segments (seg_total entries), the slot counts in flag bits 3-6, hbase, and the
 // FP64 / FP32 slot arrays. Leaves op->halo_ok false (atomics kept) when some node
 // has more than 15 foreign entries.
@@ -685,8 +685,8 @@ void build_halo_slots(geo_op* op, int64_t seg_total) {
     GEO_CUDA(cudaMemcpyAsync(&total, op->hbase.p + nch, sizeof(int), cudaMemcpyDeviceToHost, s));
     sync(ctx, "halo slots");
     if (total != A) fail(GEO_ERR_CUDA, "halo slot count mismatch");
-    op->halo64.alloc(A);
-    op->halo32.alloc(A);
+    op->halo64.alloc(A * op->dpn);
+    op->halo32.alloc(A * op->dpn);
     // slots of Dirichlet entries are never written (the node update ignores them)
     GEO_CUDA(cudaMemsetAsync(op->halo64.p, 0, op->halo64.bytes(), s));
     GEO_CUDA(cudaMemsetAsync(op->halo32.p, 0, op->halo32.bytes(), s));
@@ -836,7 +836,7 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
         check_launch(ctx, "k_patch_foreign");
         sync(ctx, "foreign segments");
         op->n_app = pf[P];
-        if (dpn == 1 && op->n_app > 0) build_halo_slots(op.get(), acc);
+        if ((dpn == 1 || dpn == 3) && op->n_app > 0) build_halo_slots(op.get(), acc);
     }
     // affine (straight-sided) elements use one metric per element
     DevBuf<int> aff(1);
@@ -863,13 +863,15 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
     with_kernels(op.get(), [&](auto k64, auto k32) {
         int per_sm = 0;
         if (op->halo[0])
-            GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_update_halo<double, false>, kNodeBS, 0));
+            GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, k_pcg_update_halo<double, decltype(k64)::DPN, false>, kNodeBS, 0));
         else
             GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                 &per_sm, k_pcg_update<double, decltype(k64)::DPN, false>, kNodeBS, 0));
         op->node_grid[0] = std::max(1, per_sm) * ctx->sm_count;
         if (op->halo[1])
-            GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_update_halo<float, true>, kNodeBS, 0));
+            GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, k_pcg_update_halo<float, decltype(k32)::DPN, true>, kNodeBS, 0));
         else
             GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                 &per_sm, k_pcg_update<float, decltype(k32)::DPN, true>, kNodeBS, 0));
@@ -940,7 +942,7 @@ template <class K, class T, bool MIXED>
 void launch_update(const geo_op* op, cudaStream_t s, const NodeArgs<T>& na) {
     constexpr int slot = std::is_same<T, double>::value ? 0 : 1;
     const unsigned g = (unsigned)op->node_grid[slot];
-    if (K::DPN == 1 && op->halo[slot]) k_pcg_update_halo<T, MIXED><<<g, kNodeBS, 0, s>>>(na);
+    if (op->halo[slot]) k_pcg_update_halo<T, K::DPN, MIXED><<<g, kNodeBS, 0, s>>>(na);
     else k_pcg_update<T, K::DPN, MIXED><<<g, kNodeBS, 0, s>>>(na);
 }
 

@@ -14,7 +14,7 @@
 //      (exact INT32 fixed point for FP32, see Scatter). Elements are ordered so
 //      a warp's 32 elements share no node, so these atomics do not collide;
 //   3. flush: a plain store for nodes no other patch touches, red.global.add
-//      for the shared ones. In the PCG mode of one-DOF operators ("halo" mode)
+//      for the shared ones. In PCG mode ("halo" mode)
 //      every own node is a plain store and every foreign node a plain store to
 //      its own slot of a halo array; the slots are numbered by owner node, so the
 //      node update adds a node's foreign contributions from consecutive slots in
@@ -68,7 +68,7 @@ struct PatchView {
     int max_for;
     int max_own;   // the largest own-node count of a patch
     int own_bulk;  // own-node slices by bulk copy (FP32 thermal PCG; the launch's shared memory holds them)
-    // halo mode (PCG, one DOF per node): the halo slot of every foreign entry, in
+    // halo mode (PCG): the halo slot of every foreign entry, in
     // the same per-patch segments as fids. halo: 0 off; 1 the slots ride in the
     // patch's bulk copy; 2 the flush reads them from global memory (coalesced), for
     // launches where the shared-memory copy would cost a resident block
@@ -168,7 +168,7 @@ struct PatchArgs {
     PcgState* st;
     double* part;  // [gridDim.x][2]
     int* err;      // DEV_ERR_* bits (bounded waits)
-    T* halo;       // halo mode: foreign contributions by slot
+    T* halo;       // halo mode: foreign contributions by slot (DPN values each)
 };
 
 // ------------------------------------------------------------------ bulk copy + mbarrier
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     using SC = Scatter<T>;
     const int M = pv.max_local * DPN;  // DOF slots of the patch-local table
     unsigned char* abuf = smem + patch_smem_fixed<K, T, NBUF>();  // NBUF x (meta | ids | flags)
-    const bool HALO = MODE == MODE_PCG && DPN == 1 && (HG != 0 || pv.halo != 0);
+    const bool HALO = MODE == MODE_PCG && (HG != 0 || pv.halo != 0);
     const int HMODE = !HALO ? 0 : (HG ? 2 : 1);  // 1: slots in shared memory, 2: from global
     const uint32_t AUX = patch_aux_bytes(pv.max_for, HMODE), AIDS = patch_aux_ids(pv.max_for);
     const uint32_t AFL = patch_aux_flags(pv.max_for);
@@ -552,11 +552,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         // 3. flush (node ids: the own range, then the foreign list still in the aux buffer)
         for (int u = threadIdx.x; u < nloc; u += blockDim.x) {
             const uint8_t fl = sfl[u];
-            if (HALO) {  // one DOF per node: own nodes stored, foreign ones to their halo slots
-                if (fl & 1) continue;
-                const T v = SC::get(ys, M, u) * invS;
-                if (u < nown) a.y[o0 + u] = v;
-                else a.halo[HG ? __ldg(pv.fslot + pm.fa + (u - nown)) : sfsl[u - nown]] = v;
+            if (HALO) {  // own nodes stored, foreign ones to their halo slots (DPN values each)
+                const int64_t base = u < nown ? (int64_t)(o0 + u) * DPN
+                                              : (int64_t)(HG ? __ldg(pv.fslot + pm.fa + (u - nown)) : sfsl[u - nown]) * DPN;
+                T* dst = u < nown ? a.y : a.halo;
+#pragma unroll
+                for (int c = 0; c < DPN; ++c)
+                    if (!((fl >> c) & 1)) dst[base + c] = SC::get(ys, M, u * DPN + c) * invS;
                 continue;
             }
             const int node = u < nown ? o0 + u : sfor[u - nown];
@@ -616,7 +618,7 @@ struct NodeArgs {
     double* w64;
     const double* b;
     int vec;  // x, r, q, dinv, pbuf0 and pbuf1 are 16-byte aligned: k_pcg_update uses 16-byte loads
-    // halo mode (one DOF per node): foreign contributions by slot; node i's slots
+    // halo mode: foreign contributions by slot (dpn values each); node i's slots
     // follow those of nodes < i, hbase[c] = slots of nodes < 32 c, flag bits 3-6 =
     // the node's slot count
     const T* halo;
@@ -897,14 +899,71 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
     pcg_update_finish<T, MIXED>(a, acc_rr, acc_rz);
 }
 
-// Node update of a one-DOF operator's PCG in halo mode (see pcg_update_halo).
-template <class T, bool MIXED>
+// Node update of a three-DOF operator in halo mode: one node per lane, its three
+// interleaved DOFs of every vector by scalar loads (issued before the slot scan),
+// then its slots' three components. A warp's 32 lanes are 32 consecutive nodes
+// starting at a multiple of 32, as in pcg_update_halo.
+template <class T>
+__device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, T cd, const T* __restrict__ p,
+                                                 T& acc_rr, T& acc_rz) {
+    const uint8_t* __restrict__ flags = a.flags;
+    const T* __restrict__ dinv = a.dinv;
+    const T* __restrict__ halo = a.halo;
+    T* __restrict__ x = a.x;
+    T* __restrict__ r = a.r;
+    const T* __restrict__ q = a.q;
+    const int lane = threadIdx.x & 31;
+    const int64_t nn = a.n / 3, nth = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd - lane < nn; nd += nth) {
+        const bool in = nd < nn;
+        T pv[3], qv[3], xv[3], rv[3], dv[3];
+        uint8_t f = 0;
+        if (in) {
+            f = flags[nd];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int64_t j = 3 * nd + c;
+                pv[c] = p[j];
+                qv[c] = q[j];
+                xv[c] = x[j];
+                rv[c] = r[j];
+                dv[c] = dinv[j];
+            }
+        }
+        const int cnt = (f >> kHaloShift) & 15;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int64_t first = __shfl_sync(0xffffffffu, nd, 0);
+        const int64_t s0 = (int64_t)a.hbase[first / 32] + (incl - cnt);
+        if (!in) continue;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            T h = T(0);
+            for (int i = 0; i < cnt; ++i) h += halo[3 * (s0 + i) + c];
+            const T qq = ((f >> c) & 1) ? cd * pv[c] : qv[c] + h;
+            const T xo = xv[c] + alpha * pv[c];
+            const T ro = rv[c] - alpha * qq;
+            x[3 * nd + c] = xo;
+            r[3 * nd + c] = ro;
+            acc_rr += ro * ro;
+            acc_rz += ro * (ro * dv[c]);
+        }
+    }
+}
+
+// Node update of a PCG in halo mode (see pcg_update_halo / pcg_update_halo3).
+template <class T, int DPN, bool MIXED>
 __global__ void __launch_bounds__(kNodeBS, kHaloMinBlocks) k_pcg_update_halo(NodeArgs<T> a) {
     PcgState* st = a.st;
     if (st->flags & (ST_DONE | ST_REFRESH)) return;
     const T* __restrict__ p = (st->it & 1) ? a.pbuf0 : a.pbuf1;
     T acc_rr = T(0), acc_rz = T(0);
-    pcg_update_halo<T, kHaloUnroll>(a, (T)st->alpha, (T)st->cd, p, acc_rr, acc_rz);
+    if (DPN == 1) pcg_update_halo<T, kHaloUnroll>(a, (T)st->alpha, (T)st->cd, p, acc_rr, acc_rz);
+    else pcg_update_halo3<T>(a, (T)st->alpha, (T)st->cd, p, acc_rr, acc_rz);
     pcg_update_finish<T, MIXED>(a, acc_rr, acc_rz);
 }
 

@@ -1,4 +1,4 @@
-"""The three ways the one-DOF PCG's patch kernel hands shared-node contributions
+"""The three ways the PCG's patch kernel hands shared-node contributions
 to the node update: red.global.add (mode 0), halo slots carried in shared memory
 (1) and halo slots read from global memory (2). The operator set-up picks one
 by occupancy (2 only on large meshes); GEO_PATCH_HALO forces each here, and the
@@ -45,3 +45,34 @@ def test_halo_modes_agree(orc, geo, n, monkeypatch):
             u, it = sols[mode, prec]
             assert np.linalg.norm(u - u0) <= 1e-9 * np.linalg.norm(u0)
             assert abs(it - it0) <= 3
+
+
+@pytest.mark.gpu
+def test_halo_modes_agree_elasticity(orc, geo, monkeypatch):
+    """The same for 3-DOF elasticity (gravity on a half-space): every mode against
+    the oracle's CG on K_bc, run to rel-res 1e-13."""
+    from test_gpu_elasticity import halfspace, setup
+    xyz, conn, mask, vals, E_e = halfspace(orc, 8, 7, 5)
+    mesh, d = setup(geo, xyz, conn, mask, vals)
+    mat = geo.IsotropicElasticity(1e11, 0.25)
+    Ko = orc.assemble_elasticity_stiffness(xyz, conn, E_e=E_e, nu=0.25)
+    fo = orc.assemble_gravity_load(xyz, conn, 3300.0, [0, 0, -9.81])
+    Kbo, fbo = orc.apply_dirichlet_bcs(Ko, fo, mask, vals)
+    ul, _ = orc.cg_solve(Kbo, fbo, max_iterations=50000, tolerance=1e-13)
+    sols = {}
+    for mode in ("0", "1", "2"):
+        monkeypatch.setenv("GEO_PATCH_HALO", mode)
+        op = geo.ElasticityOperator(mesh, d, mat, E_e)
+        for prec in ("fp64", "mixed"):
+            solver = geo.ConjugateGradient().with_max_iterations(20000).with_tolerance(1e-10).with_precision(prec)
+            u, st = op.solve(fbo, solver)
+            assert st.converged, (mode, prec)
+            assert np.linalg.norm(u - ul) <= 1e-8 * np.linalg.norm(ul), (mode, prec)
+            sols[mode, prec] = (u, st.iterations)
+        del op
+    for prec in ("fp64", "mixed"):
+        u0, it0 = sols["0", prec]
+        for mode in ("1", "2"):
+            u, it = sols[mode, prec]
+            assert np.linalg.norm(u - u0) <= 1e-9 * np.linalg.norm(u0)
+            assert abs(it - it0) <= 5
