@@ -553,6 +553,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         for (int u = threadIdx.x; u < nloc; u += blockDim.x) {
             const uint8_t fl = sfl[u];
             if (HALO) {  // own nodes stored, foreign ones to their halo slots (DPN values each)
+                if (DPN == 1) {  // kept apart: the general form costs the FP32 thermal kernel 9 registers
+                    if (fl & 1) continue;
+                    const T v = SC::get(ys, M, u) * invS;
+                    if (u < nown) a.y[o0 + u] = v;
+                    else a.halo[HG ? __ldg(pv.fslot + pm.fa + (u - nown)) : sfsl[u - nown]] = v;
+                    continue;
+                }
                 const int64_t base = u < nown ? (int64_t)(o0 + u) * DPN
                                               : (int64_t)(HG ? __ldg(pv.fslot + pm.fa + (u - nown)) : sfsl[u - nown]) * DPN;
                 T* dst = u < nown ? a.y : a.halo;
