@@ -103,6 +103,7 @@ _SIGS = {
     "geo_gmres_solve": [_P, _P, _DP, C.POINTER(CgOpts), _I32, _DP, C.POINTER(SolverStatsC)],
     "geo_direct_solve": [_P, _P, _DP, _DP, C.POINTER(SolverStatsC)],
     "geo_release_cached_memory": [],
+    "geo_device_memory_stats": [C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)],
     "geo_thermal_operator_create": [_P, _P, _P, _DP, _D, _PP],
     "geo_elasticity_operator_create": [_P, _P, _P, _DP, _D, _D, _PP],
     "geo_op_set_coefficients": [_P, _DP, _D],

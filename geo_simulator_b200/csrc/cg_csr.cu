@@ -276,7 +276,10 @@ int geo_cg_solve(geo_ctx* ctx, const geo_csr* A, const double* b, const geo_cg_o
 //  * the first call on a device looks the array up with cudaGetSymbolAddress,
 //    which can make the runtime load this module and reserve the array; make
 //    that first call before the phase that must not allocate, and before any
-//    stream capture begins.
+//    stream capture begins. The address is kept per device together with the
+//    driver's unique id of the device's current context; after a
+//    cudaDeviceReset the context (and its id) is new, so the next call looks the
+//    array up again instead of using an address of the old context.
 namespace geo {
 namespace {
 
@@ -296,17 +299,48 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+unsigned long long g_noalloc_ctx_id[kNoAllocMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on `device` (which must be current).
+// Unique id of the calling thread's current driver context (cuCtxGetId through
+// the runtime's driver entry point, so the library needs no -lcuda); 0 when the
+// driver cannot say, in which case the cached address is trusted as before.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    void* c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == 0 && c && get_id(c, &id) == 0) return id;
+    return 0;
+}
+
+// Device address of g_noalloc_scratch on `device` (which must be current),
+// looked up once per device and context.
 unsigned char* noalloc_scratch(int device) {
     if (device < 0 || device >= kNoAllocMaxDevices) fail(GEO_ERR_UNSUPPORTED, "device ordinal out of range");
+    const unsigned long long ctx_id = current_context_id();
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[device]) {
+    if (!g_noalloc_addr[device] || g_noalloc_ctx_id[device] != ctx_id) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             fail(GEO_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
         g_noalloc_addr[device] = static_cast<unsigned char*>(p);
+        g_noalloc_ctx_id[device] = ctx_id;
     }
     return g_noalloc_addr[device];
 }

@@ -924,86 +924,88 @@ __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, 
     const int lane = threadIdx.x & 31;
     const int64_t nn = a.n / 3, nth = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (std::is_same<T, float>::value && a.vec) {
-        // FP32: two consecutive nodes per lane, so that each vector's six values are
-        // three 8-byte loads (a lane's pair starts at DOF 6 m); a warp covers 64
-        // nodes starting at a multiple of 64
-        const int64_t np2 = nn / 2;
-        for (int64_t m = tid; m - lane < np2; m += nth) {
-            const bool in = m < np2;
-            float pv[6], qv[6], xv[6], rv[6], dv[6];
-            uint8_t f[2] = {0, 0};
-            if (in) {
-                f[0] = flags[2 * m];
-                f[1] = flags[2 * m + 1];
-#pragma unroll
+    if constexpr (std::is_same_v<T, float>) {
+        if (a.vec) {
+            // FP32: two consecutive nodes per lane, so that each vector's six values are
+            // three 8-byte loads (a lane's pair starts at DOF 6 m); a warp covers 64
+            // nodes starting at a multiple of 64
+            const int64_t np2 = nn / 2;
+            for (int64_t m = tid; m - lane < np2; m += nth) {
+                const bool in = m < np2;
+                float pv[6], qv[6], xv[6], rv[6], dv[6];
+                uint8_t f[2] = {0, 0};
+                if (in) {
+                    f[0] = flags[2 * m];
+                    f[1] = flags[2 * m + 1];
+    #pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const float2 tp = reinterpret_cast<const float2*>(p)[3 * m + k];
+                        const float2 tq = reinterpret_cast<const float2*>(q)[3 * m + k];
+                        const float2 tx = reinterpret_cast<const float2*>(x)[3 * m + k];
+                        const float2 tr = reinterpret_cast<const float2*>(r)[3 * m + k];
+                        const float2 td = reinterpret_cast<const float2*>(dinv)[3 * m + k];
+                        pv[2 * k] = tp.x, pv[2 * k + 1] = tp.y;
+                        qv[2 * k] = tq.x, qv[2 * k + 1] = tq.y;
+                        xv[2 * k] = tx.x, xv[2 * k + 1] = tx.y;
+                        rv[2 * k] = tr.x, rv[2 * k + 1] = tr.y;
+                        dv[2 * k] = td.x, dv[2 * k + 1] = td.y;
+                    }
+                }
+                const int c0 = (f[0] >> kHaloShift) & 15, c1 = (f[1] >> kHaloShift) & 15;
+                const int tot = c0 + c1;
+                int incl = tot;
+    #pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int64_t first = __shfl_sync(0xffffffffu, m, 0) * 2;
+                const int64_t s0 = (int64_t)a.hbase[first / 32] + (incl - tot);
+                if (!in) continue;
+    #pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int cnt = e ? c1 : c0;
+                    const int64_t se = s0 + (e ? c0 : 0);
+    #pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int v = 3 * e + c;
+                        float h = 0.0f;
+                        for (int i = 0; i < cnt; ++i) h += halo[3 * (se + i) + c];
+                        const float qq = ((f[e] >> c) & 1) ? (float)cd * pv[v] : qv[v] + h;
+                        xv[v] = xv[v] + (float)alpha * pv[v];
+                        rv[v] = rv[v] - (float)alpha * qq;
+                        acc_rr += rv[v] * rv[v];
+                        acc_rz += rv[v] * (rv[v] * dv[v]);
+                    }
+                }
+    #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    const float2 tp = reinterpret_cast<const float2*>(p)[3 * m + k];
-                    const float2 tq = reinterpret_cast<const float2*>(q)[3 * m + k];
-                    const float2 tx = reinterpret_cast<const float2*>(x)[3 * m + k];
-                    const float2 tr = reinterpret_cast<const float2*>(r)[3 * m + k];
-                    const float2 td = reinterpret_cast<const float2*>(dinv)[3 * m + k];
-                    pv[2 * k] = tp.x, pv[2 * k + 1] = tp.y;
-                    qv[2 * k] = tq.x, qv[2 * k + 1] = tq.y;
-                    xv[2 * k] = tx.x, xv[2 * k + 1] = tx.y;
-                    rv[2 * k] = tr.x, rv[2 * k + 1] = tr.y;
-                    dv[2 * k] = td.x, dv[2 * k + 1] = td.y;
+                    reinterpret_cast<float2*>(x)[3 * m + k] = make_float2(xv[2 * k], xv[2 * k + 1]);
+                    reinterpret_cast<float2*>(r)[3 * m + k] = make_float2(rv[2 * k], rv[2 * k + 1]);
                 }
             }
-            const int c0 = (f[0] >> kHaloShift) & 15, c1 = (f[1] >> kHaloShift) & 15;
-            const int tot = c0 + c1;
-            int incl = tot;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            const int64_t first = __shfl_sync(0xffffffffu, m, 0) * 2;
-            const int64_t s0 = (int64_t)a.hbase[first / 32] + (incl - tot);
-            if (!in) continue;
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int cnt = e ? c1 : c0;
-                const int64_t se = s0 + (e ? c0 : 0);
-#pragma unroll
+            // an odd last node: its first slot from the 32-node chunk start
+            for (int64_t nd = 2 * np2 + tid; nd < nn; nd += nth) {
+                const uint8_t f = flags[nd];
+                const int cnt = (f >> kHaloShift) & 15;
+                int64_t s0 = a.hbase[nd / 32];
+                for (int64_t i = nd & ~(int64_t)31; i < nd; ++i) s0 += (flags[i] >> kHaloShift) & 15;
+    #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const int v = 3 * e + c;
-                    float h = 0.0f;
-                    for (int i = 0; i < cnt; ++i) h += halo[3 * (se + i) + c];
-                    const float qq = ((f[e] >> c) & 1) ? (float)cd * pv[v] : qv[v] + h;
-                    xv[v] = xv[v] + (float)alpha * pv[v];
-                    rv[v] = rv[v] - (float)alpha * qq;
-                    acc_rr += rv[v] * rv[v];
-                    acc_rz += rv[v] * (rv[v] * dv[v]);
+                    const int64_t j = 3 * nd + c;
+                    T h = T(0);
+                    for (int i = 0; i < cnt; ++i) h += halo[3 * (s0 + i) + c];
+                    const T qq = ((f >> c) & 1) ? cd * p[j] : q[j] + h;
+                    const T xo = x[j] + alpha * p[j];
+                    const T ro = r[j] - alpha * qq;
+                    x[j] = xo;
+                    r[j] = ro;
+                    acc_rr += ro * ro;
+                    acc_rz += ro * (ro * dinv[j]);
                 }
             }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                reinterpret_cast<float2*>(x)[3 * m + k] = make_float2(xv[2 * k], xv[2 * k + 1]);
-                reinterpret_cast<float2*>(r)[3 * m + k] = make_float2(rv[2 * k], rv[2 * k + 1]);
-            }
+            return;
         }
-        // an odd last node: its first slot from the 32-node chunk start
-        for (int64_t nd = 2 * np2 + tid; nd < nn; nd += nth) {
-            const uint8_t f = flags[nd];
-            const int cnt = (f >> kHaloShift) & 15;
-            int64_t s0 = a.hbase[nd / 32];
-            for (int64_t i = nd & ~(int64_t)31; i < nd; ++i) s0 += (flags[i] >> kHaloShift) & 15;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const int64_t j = 3 * nd + c;
-                T h = T(0);
-                for (int i = 0; i < cnt; ++i) h += halo[3 * (s0 + i) + c];
-                const T qq = ((f >> c) & 1) ? cd * p[j] : q[j] + h;
-                const T xo = x[j] + alpha * p[j];
-                const T ro = r[j] - alpha * qq;
-                x[j] = xo;
-                r[j] = ro;
-                acc_rr += ro * ro;
-                acc_rz += ro * (ro * dinv[j]);
-            }
-        }
-        return;
     }
     for (int64_t nd = tid; nd - lane < nn; nd += nth) {
         const bool in = nd < nn;

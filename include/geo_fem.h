@@ -99,6 +99,10 @@ const char* geo_version(void);
  * kept memory of every device to the driver; geo_ctx_destroy does so for its
  * device, and an allocation that runs out of memory does so before retrying. */
 int geo_release_cached_memory(void);
+/* No counterpart in the reference. Counters of the library's device allocator:
+ * bytes handed out and not yet freed, bytes kept for reuse, and the number of
+ * cudaMalloc calls it has made since the process started (any pointer may be NULL). */
+int geo_device_memory_stats(int64_t* live_bytes, int64_t* cached_bytes, int64_t* cuda_mallocs);
 int geo_sm_count(const geo_ctx* ctx, int* sm_count);
 /* The context's CUDA stream (cudaStream_t), so callers can order or time their
  * own work against the library's launches. */

@@ -29,6 +29,13 @@ def _noalloc(geo, A, b_ptr, x_ptr, solver):
     return code, st
 
 
+def _mallocs():
+    from geo_simulator_b200 import _native as N
+    live, cached, n = C.c_int64(), C.c_int64(), C.c_int64()
+    assert N.lib().geo_device_memory_stats(C.byref(live), C.byref(cached), C.byref(n)) == N.GEO_OK
+    return live.value, cached.value, n.value
+
+
 def test_noalloc_matches_cg_solve_on_two_calls(orc, geo):
     import torch
     from geo_simulator_b200 import _native as N
@@ -37,15 +44,26 @@ def test_noalloc_matches_cg_solve_on_two_calls(orc, geo):
     x_ref, st_ref = solver.solve(Kb, fb)
     assert st_ref.converged
     b = torch.from_numpy(fb).cuda()
+    xs = [torch.full_like(b, float("nan")) for _ in range(2)]
     for call in range(2):
-        x = torch.full_like(b, float("nan"))
+        x = xs[call]
         torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        stats0 = _mallocs()
         code, st = _noalloc(geo, Kb, b.data_ptr(), x.data_ptr(), solver)
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        stats1 = _mallocs()
         assert code == N.GEO_OK, N.lib().geo_last_error(Kb.ctx.h)
         # same kernel, same grid, fixed-order reductions: bit-identical
         assert np.array_equal(x.cpu().numpy(), x_ref), call
         assert st.iterations == st_ref.iterations and st.converged == 1
         assert st.residual_norm == st_ref.residual_norm
+        if call == 1:
+            # the call after the first takes no device memory: the driver's free
+            # memory and the library allocator's counters are unchanged across it
+            assert free1 == free0, (free0, free1)
+            assert stats1 == stats0, (stats0, stats1)
 
 
 def test_noalloc_not_converged_matches(orc, geo):
