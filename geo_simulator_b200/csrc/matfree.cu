@@ -559,6 +559,10 @@ int setup_patch_nbuf(size_t attr_bytes, size_t plain, size_t own, int& per_sm_pl
                                   (int)attr_bytes));
     GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_PCG, NBUF, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)attr_bytes));
+    GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_FREE, NBUF, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)attr_bytes));
+    GEO_CUDA(cudaFuncSetAttribute(k_patch<K, T, MODE_LIFT, NBUF, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)attr_bytes));
     per_sm_plain = 0;
     GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_plain, k_patch<K, T, MODE_PCG, NBUF>, kPatchBS,
                                                            plain));
@@ -627,9 +631,9 @@ void launch_patch(const geo_op* op, int slot, cudaStream_t s, const T* qd, const
     const unsigned g = (unsigned)std::min(op->patch_grid[slot], op->n_patches);
     PatchView v = view(op);
     v.own_bulk = op->own_bulk[slot];
-    v.halo = MODE == MODE_PCG ? op->halo[slot] : 0;
+    v.halo = pa.halo ? op->halo[slot] : 0;  // halo mode whenever the caller passes the slot array
     const size_t smem = op->patch_smem[slot];
-    const bool hg = MODE == MODE_PCG && v.halo == 2;
+    const bool hg = v.halo == 2;
     if (op->nbuf[slot] == 2) {
         if (hg) k_patch<K, T, MODE, 2, 1><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
         else k_patch<K, T, MODE, 2><<<g, kPatchBS, smem, s>>>(v, qd, (T)op->cl, (T)op->cm, pa);
@@ -893,6 +897,7 @@ void apply_new(geo_op* op, const T* x, T* y, int mode) {
     cudaStream_t s = ctx->stream;
     GEO_CUDA(cudaMemsetAsync(y, 0, op->ndof * sizeof(T), s));
     constexpr bool dbl = std::is_same<T, double>::value;
+    const bool halo = op->halo[dbl ? 0 : 1] != 0;
     reset_dev_err(ctx);
     with_kernels(op, [&](auto k64, auto k32) {
         using K = typename std::conditional<dbl, decltype(k64), decltype(k32)>::type;
@@ -901,11 +906,17 @@ void apply_new(geo_op* op, const T* x, T* y, int mode) {
         pa.x = x;
         pa.y = y;
         pa.err = ctx->dev_err.p;
+        if (halo) pa.halo = dbl ? (T*)op->halo64.p : (T*)op->halo32.p;
         if (mode == MODE_FREE) launch_patch<K, T, MODE_FREE>(op, dbl ? 0 : 1, s, qd, pa);
         else launch_patch<K, T, MODE_LIFT>(op, dbl ? 0 : 1, s, qd, pa);
     });
     check_launch(ctx, "k_patch");
-    if (mode == MODE_FREE) {
+    if (halo) {  // foreign contributions in slot order (and the Dirichlet rows of FREE)
+        const T* h = dbl ? (const T*)op->halo64.p : (const T*)op->halo32.p;
+        k_halo_combine<T><<<nblk(op->N), kNodeBS, 0, s>>>(op->flags.p, op->hbase.p, h, op->dpn, op->N, op->cd, x,
+                                                          y, mode == MODE_FREE);
+        check_launch(ctx, "k_halo_combine");
+    } else if (mode == MODE_FREE) {
         k_dir_rows<T><<<nblk(op->ndof), 256, 0, s>>>(op->flags.p, op->dpn, op->ndof, op->cd, x, y);
         check_launch(ctx, "k_dir_rows");
     }
@@ -1014,6 +1025,8 @@ PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
     if (op->halo[0]) {
         n64.halo = p64.halo = op->halo64.p;
         n64.hbase = op->hbase.p;
+        n32.halo64 = op->halo64.p;  // the mixed solver's FP64 refresh apply
+        n32.hbase = op->hbase.p;
     }
     if (op->halo[1]) {
         n32.halo = p32.halo = op->halo32.p;
@@ -1098,11 +1111,13 @@ int solve_new(geo_op* op, const geo_cg_opts& o, geo_solver_stats* st) {
             ra.x = x_new;
             ra.y = op->w64.p;
             ra.err = &op->state.p->err;
+            if (op->halo[0]) ra.halo = op->halo64.p;  // fixed-order foreign sums: bit-reproducible refresh
             k_refresh_flush<<<ng, kNodeBS, 0, s>>>(n32);
             with_kernels(op, [&](auto k64, auto) {
                 launch_patch<decltype(k64), double, MODE_FREE>(op, 0, s, op->qd64.p, ra);
             });
-            k_refresh_residual<<<ng, kNodeBS, 0, s>>>(n32);
+            if (op->halo[0]) k_refresh_residual_halo<<<ng, kNodeBS, 0, s>>>(n32);
+            else k_refresh_residual<<<ng, kNodeBS, 0, s>>>(n32);
             k_refresh_rescale<<<ng, kNodeBS, 0, s>>>(n32);
             check_launch(ctx, "refresh");
             launches += 4;

@@ -14,11 +14,13 @@
 //      (exact INT32 fixed point for FP32, see Scatter). Elements are ordered so
 //      a warp's 32 elements share no node, so these atomics do not collide;
 //   3. flush: a plain store for nodes no other patch touches, red.global.add
-//      for the shared ones. In PCG mode ("halo" mode)
-//      every own node is a plain store and every foreign node a plain store to
-//      its own slot of a halo array; the slots are numbered by owner node, so the
-//      node update adds a node's foreign contributions from consecutive slots in
-//      a fixed order. The PCG loop then issues no global atomics.
+//      for the shared ones. In "halo" mode (every mode, when the operator has
+//      halo slots) every own node is a plain store and every foreign node a
+//      plain store to its own slot of a halo array; the slots are numbered by
+//      owner node, so the node update (PCG) or k_halo_combine (operator apply,
+//      lift) adds a node's foreign contributions from consecutive slots in a
+//      fixed order. No global atomics are issued and results are bit-identical
+//      from run to run.
 // In PCG mode step 1 also forms the new search direction p = z + beta p_old
 // (z = D^-1 r) on the fly: the Jacobi scaling and the p-update ride on the
 // operator's gather. p is double-buffered by iteration parity.
@@ -296,7 +298,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     using SC = Scatter<T>;
     const int M = pv.max_local * DPN;  // DOF slots of the patch-local table
     unsigned char* abuf = smem + patch_smem_fixed<K, T, NBUF>();  // NBUF x (meta | ids | flags)
-    const bool HALO = MODE == MODE_PCG && (HG != 0 || pv.halo != 0);
+    const bool HALO = HG != 0 || pv.halo != 0;
     const int HMODE = !HALO ? 0 : (HG ? 2 : 1);  // 1: slots in shared memory, 2: from global
     const uint32_t AUX = patch_aux_bytes(pv.max_for, HMODE), AIDS = patch_aux_ids(pv.max_for);
     const uint32_t AFL = patch_aux_flags(pv.max_for);
@@ -632,6 +634,7 @@ struct NodeArgs {
     // the node's slot count
     const T* halo;
     const int32_t* hbase;
+    const double* halo64;  // mixed refresh: FP64 slots of the FP64 apply (halo mode)
 };
 
 // 16-byte vector of T
@@ -1197,6 +1200,103 @@ __global__ void __launch_bounds__(kNodeBS) k_refresh_residual(NodeArgs<float> a)
             } else {
                 st->ratio = st->s_scale / s_new;
             }
+        }
+    }
+}
+
+// Sum over the warp of lanes' slot counts before this lane: the exclusive prefix
+// that, added to hbase[node / 32], gives the node's first halo slot. Every lane of
+// the warp calls it; the warp's lanes hold 32 consecutive nodes from a multiple of
+// 32 (lanes past the end pass cnt = 0).
+__device__ __forceinline__ int halo_prefix(int cnt, int lane) {
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    return incl - cnt;
+}
+
+// MIXED refresh 3, halo mode: as k_refresh_residual, with K x64 on free rows =
+// (own-patch sum in w) + (the node's FP64 halo slots, in slot order). Threads
+// take nodes; the grid is a multiple of 32 threads, so warps cover aligned
+// 32-node chunks and the loop condition is warp-uniform.
+__global__ void __launch_bounds__(kNodeBS) k_refresh_residual_halo(NodeArgs<float> a) {
+    PcgState* st = a.st;
+    const double cd = st->cd;
+    const int dpn = a.dpn, lane = threadIdx.x & 31;
+    const int64_t nn = a.n / dpn, nth = (int64_t)gridDim.x * blockDim.x;
+    double rr = 0.0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j - lane < nn; j += nth) {
+        const bool in = j < nn;
+        const uint8_t f = in ? a.flags[j] : (uint8_t)0;
+        const int cnt = (f >> kHaloShift) & 15;
+        const int pre = halo_prefix(cnt, lane);
+        if (!in) continue;
+        const int64_t s0 = (int64_t)a.hbase[j >> 5] + pre;
+        for (int c = 0; c < dpn; ++c) {
+            const int64_t i = j * dpn + c;
+            double kx;
+            if ((f >> c) & 1) {
+                kx = cd * a.x64[i];
+            } else {
+                kx = a.w64[i];
+                for (int k = 0; k < cnt; ++k) kx += a.halo64[(s0 + k) * dpn + c];
+            }
+            const double ri = a.b[i] - kx;
+            a.w64[i] = ri;
+            rr += ri * ri;
+        }
+    }
+    double v[1] = {rr};
+    store_partial<1>(a.part, v);
+    if (last_block(&st->ticket[TICKET_AUX])) {
+        double t[1];
+        grid_total<1>(a.part, gridDim.x, t);
+        if (threadIdx.x == 0) {
+            st->ticket[TICKET_AUX] = 0;
+            const double s_new = sqrt(t[0]);
+            st->nupd += 1;
+            st->res = s_new;
+            st->s_new = s_new;
+            if (s_new < st->tol * st->bnorm || s_new < st->abs_tol) {
+                st->flags = (st->flags & ~ST_REFRESH) | ST_DONE | ST_CONVERGED;
+            } else {
+                st->ratio = st->s_scale / s_new;
+            }
+        }
+    }
+}
+
+// After a FREE or LIFT pass in halo mode: y_j += node j's halo slots (slot order)
+// on free rows; with `dir_rows`, Dirichlet rows y = cd x (as k_dir_rows). Node-
+// per-thread with warp-aligned 32-node chunks (grid a multiple of 32 threads).
+template <class T>
+__global__ void __launch_bounds__(kNodeBS) k_halo_combine(const uint8_t* __restrict__ flags,
+                                                          const int32_t* __restrict__ hbase,
+                                                          const T* __restrict__ halo, int dpn, int64_t nn,
+                                                          double cd, const T* __restrict__ x, T* __restrict__ y,
+                                                          int dir_rows) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j - lane < nn; j += nth) {
+        const bool in = j < nn;
+        const uint8_t f = in ? flags[j] : (uint8_t)0;
+        const int cnt = (f >> kHaloShift) & 15;
+        const int pre = halo_prefix(cnt, lane);
+        if (!in) continue;
+        const int64_t s0 = (int64_t)hbase[j >> 5] + pre;
+        for (int c = 0; c < dpn; ++c) {
+            const int64_t i = j * dpn + c;
+            if ((f >> c) & 1) {
+                if (dir_rows) y[i] = (T)(cd * (double)x[i]);
+                continue;
+            }
+            if (cnt == 0) continue;
+            T h = y[i];
+            for (int k = 0; k < cnt; ++k) h += halo[(s0 + k) * dpn + c];
+            y[i] = h;
         }
     }
 }

@@ -40,17 +40,43 @@ import numpy as np
 LX, LY, LZ = 1000.0, 1000.0, 600.0
 
 
+# qdata values per element of the affine operators: thermal G (6), elasticity J^-1 and s (10)
+NQD = {1: 6, 3: 10}
+
+
 def patch_pcg_bytes(E, N, s, dpn=1):
-    """Algorithmic bytes of one PCG-mode patch-kernel launch: per element 10 int32
-    node ids and its coefficient; per node 3 coordinates, then per DOF r, D^-1 and
-    the previous p read, the new p and q = K p written; the Dirichlet bitmask."""
-    return E * (10 * 4 + s) + N * 3 * s + N * dpn * 5 * s + N * dpn / 8
+    """Bytes one PCG-mode patch-kernel launch must move: per element its paired
+    16-bit patch-local connectivity (20 B) and its qdata (6 or 10 values of s
+    bytes); per DOF r, D^-1 and the previous p read, the new p and q = K p written;
+    the Dirichlet bitmask. (The node coordinates are not read: the operator stores
+    qdata instead.)"""
+    return E * (20 + NQD[dpn] * s) + N * dpn * 5 * s + N / 8
 
 
 def update_bytes(N, s, dpn=1):
     """Algorithmic bytes of one node-update launch: p, q, x, r, D^-1 read, x and r
     written, Dirichlet bitmask."""
     return N * dpn * 7 * s + N * dpn / 8
+
+
+# Floating-point operations per element of one PCG-mode patch-kernel launch,
+# counted from the kernels' own formulation (matfree.cuh, mf_kernels.cuh; an FMA
+# counts two): thermal ThermalK::apply 186 (vertex sums 20, four quadrature points
+# 124, outputs 42), the element's share of p.Kp 20, the fixed-point scale 10;
+# elasticity ElasticK::apply 1092 (vertex sums 60, four quadrature points x 258:
+# displacement gradient 78, trace 3, stress 30, its transpose back to the 30 DOFs
+# 147), p.Kp 60, scale 30. Per DOF the gather forms p = D^-1 r + beta p_old (3).
+PATCH_FLOPS_PER_ELEMENT = {1: 216, 3: 1182}
+
+
+def patch_pcg_flops(E, N, dpn=1):
+    return E * PATCH_FLOPS_PER_ELEMENT[dpn] + 3 * N * dpn
+
+
+def cuda_core_peak_tflops(sm_mhz, fp64=False, sms=148):
+    """Nominal CUDA-core peak of a B200 at the given SM clock: 128 FP32 (64 FP64)
+    FMA lanes per SM, two flops per FMA."""
+    return sms * (64 if fp64 else 128) * 2 * sm_mhz * 1e6 / 1e12
 
 
 def meshgen_bytes(n_nodes, n_elem, n_vertices):

@@ -497,6 +497,19 @@ int orc_gravity_load(const double nodes[30], double rho, const double g[3], doub
     return gravity_load(nodes, rho, g, fe) ? 1 : 0;
 }
 
+int orc_thermal_stiffness_all(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn,
+                              const double* k_e, double k, double* Ke) {
+    (void)n_nodes;
+    int ok = 1;
+#pragma omp parallel for schedule(static) reduction(&& : ok)
+    for (int64_t e = 0; e < n_elem; ++e) {
+        double nodes[30];
+        gather_nodes(xyz, conn, e, nodes);
+        ok = ok && thermal_stiffness(nodes, k_e ? k_e[e] : k, Ke + (size_t)e * 100);
+    }
+    return ok;
+}
+
 // ================================================================ assembly
 // assembly.rs:69-117 (parallel) and :22-58 (serial). Rows/cols are node ids.
 orc_csr* orc_assemble_thermal_stiffness(int64_t n_nodes, const double* xyz, int64_t n_elem,

@@ -58,6 +58,11 @@ int orc_thermal_load(const double nodes[30], double Q, double fe[10]);
 void orc_constitutive_matrix(double E, double nu, double D[36]);
 void orc_b_matrix(const double dNdx[30], double B[180]);
 int orc_elasticity_stiffness(const double nodes[30], double E, double nu, double Ke[900]);
+/* element.rs:23-61 for every element of a mesh (OpenMP over elements, as the
+ * rayon loop of assembly.rs:69-117): Ke[e][10][10]; k_e per element, or k when
+ * k_e is NULL. Returns 0 on a singular Jacobian. */
+int orc_thermal_stiffness_all(int64_t n_nodes, const double* xyz, int64_t n_elem, const int64_t* conn,
+                              const double* k_e, double k, double* Ke);
 int orc_gravity_load(const double nodes[30], double rho, const double g[3], double fe[30]);
 
 /* ---- assembly: assembly.rs:22-230, 389-437, 906-937 ---- */

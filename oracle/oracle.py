@@ -67,6 +67,7 @@ def _declare(L):
         "orc_element_volume": (C.c_double, [_D]),
         "orc_quadrature": (C.c_int, [C.c_int, _D, _D]),
         "orc_thermal_stiffness": (C.c_int, [_D, C.c_double, _D]),
+        "orc_thermal_stiffness_all": (C.c_int, [C.c_int64, _D, C.c_int64, _I64, _D, C.c_double, _D]),
         "orc_thermal_mass": (C.c_int, [_D, C.c_double, C.c_double, _D]),
         "orc_thermal_load": (C.c_int, [_D, C.c_double, _D]),
         "orc_constitutive_matrix": (None, [C.c_double, C.c_double, _D]),
@@ -200,6 +201,16 @@ def thermal_stiffness(nodes, k):
     if not lib().orc_thermal_stiffness(_d(_f64(nodes)), k, _d(out)):
         raise ZeroDivisionError("Singular Jacobian")
     return out.reshape(10, 10)
+
+
+def thermal_stiffness_all(xyz, conn, k=1.0, k_e=None):
+    """element.rs:23-61 for every element (OpenMP): array [E][10][10]."""
+    xyz, conn = _f64(xyz), _i64(conn)
+    out = np.empty((conn.shape[0], 10, 10))
+    ke = _d(_f64(k_e)) if k_e is not None else None
+    if not lib().orc_thermal_stiffness_all(xyz.shape[0], _d(xyz), conn.shape[0], _i(conn), ke, float(k), _d(out)):
+        raise ZeroDivisionError("Singular Jacobian")
+    return out
 
 
 def thermal_mass(nodes, rho, cp):

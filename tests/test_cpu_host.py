@@ -92,16 +92,40 @@ def test_seeded_fields_are_deterministic():
     assert c.size == 1000 and np.unique(c).size == 1000 and c.max() < 5000
 
 
-def test_bench_byte_model():
+def test_bench_byte_and_flop_model():
     import bench
+    from geo_simulator_b200 import kernel_timing as kt
     E, N = 12582912, 16974593
-    # apply bytes of the 128^3 FP32 operator: E(40 + 4) + N(12 + 4 + 4) + N/8
-    assert bench.apply_bytes(E, N, 4) == pytest.approx(E * 44 + N * 20 + N / 8)
-    # PCG-mode patch launch: E(40 + 4) + N(12 + 3*4 + 2*4) + N/8; node update: 7 N 4 + N/8
-    assert bench.patch_pcg_bytes(E, N, 4) == pytest.approx(E * 44 + N * 32 + N / 8)
-    assert bench.update_bytes(N, 4) == pytest.approx(28 * N + N / 8)
+    # plain apply (int32 connectivity, k_e, coordinates): E(40 + 4) + N(12 + 4 + 4) + N/8
+    assert bench.survey_apply_bytes(E, N, 4) == pytest.approx(E * 44 + N * 20 + N / 8)
+    # PCG-mode patch launch, what it must move: 16-bit connectivity 20 B and G 6 x 4 B per
+    # element, r / D^-1 / p_old in and p / q out per DOF, bitmask
+    assert kt.patch_pcg_bytes(E, N, 4) == pytest.approx(E * 44 + N * 20 + N / 8)
+    assert kt.patch_pcg_bytes(E, N, 8, 3) == pytest.approx(E * (20 + 80) + N * 3 * 40 + N / 8)
+    assert kt.update_bytes(N, 4) == pytest.approx(28 * N + N / 8)
     assert bench.solve_bytes(E, N, 10, 1) == pytest.approx(
-        10 * (bench.patch_pcg_bytes(E, N, 4) + bench.update_bytes(N, 4)) + bench.apply_bytes(E, N, 8) + 32 * N)
+        10 * (kt.patch_pcg_bytes(E, N, 4) + kt.update_bytes(N, 4)) + E * 68 + 16 * N + N / 8 + 32 * N)
+    # FLOPs per element from the kernels' formulation; CUDA-core peaks at 1965 MHz
+    assert kt.patch_pcg_flops(E, N) == E * 216 + 3 * N
+    assert kt.patch_pcg_flops(E, N, 3) == E * 1182 + 9 * N
+    assert kt.cuda_core_peak_tflops(1965.0) == pytest.approx(74.45, rel=1e-3)
+    assert kt.cuda_core_peak_tflops(1965.0, fp64=True) == pytest.approx(37.22, rel=1e-3)
+    assert bench.cube_counts(128) == (12582912, 16974593)
+    assert bench.cube_counts(48, 32) == (442368, 611585)
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """The reference arm builds its inputs with the oracle's generate_cube: importing
+    the package's numpy field helper must not load libgeofem.so."""
+    import subprocess
+    import sys
+    code = ("import bench; xyz, conn, k, m, v = bench.oracle_inputs(2); "
+            "maps = open('/proc/self/maps').read(); "
+            "assert 'libgeofem' not in maps and 'liboracle' in maps; print(conn.shape[0])")
+    out = subprocess.run([sys.executable, "-c", code], cwd=os.path.dirname(os.path.dirname(__file__)),
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == "48"
 
 
 def _gloo_worker(rank, world, port, out):
