@@ -73,6 +73,23 @@ __global__ void conn_to_soa(const int32_t* __restrict__ aos, int32_t* __restrict
 }
 
 }  // namespace
+
+void ctx_retain(geo_ctx* c) { c->refs.fetch_add(1, std::memory_order_relaxed); }
+
+void ctx_release(geo_ctx* c) {
+    if (c->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    const int dev = c->device;
+    cudaSetDevice(dev);
+    cudaStreamSynchronize(c->stream);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    dev_release_cached(dev);
+    if (cur >= 0 && cur != dev) cudaSetDevice(cur);
+}
 }  // namespace geo
 
 using namespace geo;
@@ -125,14 +142,7 @@ int geo_ctx_destroy(geo_ctx* ctx) {
     if (!ctx) return GEO_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    ctx->dev_err.release();
-    for (auto& b : ctx->scratch) b.release();
-    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
-    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
-    const int dev = ctx->device;
-    delete ctx;
-    geo::dev_release_cached(dev);
+    geo::ctx_release(ctx);  // freed now, or when the last object made on it is destroyed
     return GEO_OK;
 }
 
@@ -161,6 +171,7 @@ int geo_mesh_create(geo_ctx* ctx, int64_t n_nodes, const double* xyz, int64_t n_
     GEO_CHECK_ARG(xyz && conn, "xyz/conn is NULL");
     auto m = std::make_unique<geo_mesh>();
     m->ctx = ctx;
+    m->ref.set(ctx);
     m->n_nodes = n_nodes;
     m->n_elem = n_elem;
     cudaStream_t s = ctx->stream;
@@ -197,6 +208,7 @@ int geo_dofs_create(geo_ctx* ctx, int64_t n_nodes, int32_t dofs_per_node, const 
     GEO_CHECK_ARG(dofs_per_node >= 1 && dofs_per_node <= 3, "dofs_per_node must be 1..3");
     auto d = std::make_unique<geo_dofs>();
     d->ctx = ctx;
+    d->ref.set(ctx);
     d->n_nodes = n_nodes;
     d->dpn = dofs_per_node;
     d->n_dofs = n_nodes * dofs_per_node;

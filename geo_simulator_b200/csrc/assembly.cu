@@ -371,6 +371,7 @@ namespace {
 std::unique_ptr<geo_csr> new_csr(geo_ctx* ctx, int64_t rows, int64_t cols, int64_t nnz) {
     auto A = std::make_unique<geo_csr>();
     A->ctx = ctx;
+    A->ref.set(ctx);
     A->n_rows = rows;
     A->n_cols = cols;
     A->nnz = nnz;

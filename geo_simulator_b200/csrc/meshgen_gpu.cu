@@ -316,6 +316,7 @@ int geo_mesh_generate_cube(geo_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, dou
     if (g.nv + n_mid != n_nodes) fail(GEO_ERR_UNSUPPORTED, "internal: cube midpoint count mismatch");
     auto m = std::make_unique<geo_mesh>();
     m->ctx = ctx;
+    m->ref.set(ctx);
     m->n_nodes = n_nodes;
     m->n_elem = n_elem;
     m->xyz.alloc(3 * n_nodes);

@@ -1,6 +1,7 @@
 // Internal definitions of the opaque C-ABI objects and the cross-file helpers.
 #pragma once
 
+#include <atomic>
 #include <memory>
 #include <string>
 #include <vector>
@@ -27,10 +28,37 @@ struct geo_ctx {
     // single calls for up to a second. Held until the context is destroyed.
     geo::DevBuf<unsigned char> scratch[geo::kScratchSlots];
     geo::HostBuf<char> pinned[2];
+    // references: the creator's (dropped by geo_ctx_destroy) plus one per live object
+    // made on this context (meshes, DOF sets, matrices, operators)
+    std::atomic<int> refs{1};
 };
+
+namespace geo {
+void ctx_retain(geo_ctx* c);
+// Drops one reference; the last one destroys the stream and events and frees the context.
+void ctx_release(geo_ctx* c);
+// The reference an object holds on the context it was made on: the context stays
+// valid until the caller destroyed it and every object made on it is gone, in
+// whatever order the caller (or a garbage collector) destroys them.
+struct CtxRef {
+    geo_ctx* c = nullptr;
+    CtxRef() = default;
+    CtxRef(const CtxRef&) = delete;
+    CtxRef& operator=(const CtxRef&) = delete;
+    void set(geo_ctx* x) {
+        if (x) ctx_retain(x);
+        if (c) ctx_release(c);
+        c = x;
+    }
+    ~CtxRef() {
+        if (c) ctx_release(c);
+    }
+};
+}  // namespace geo
 
 struct geo_mesh {
     geo_ctx* ctx = nullptr;
+    geo::CtxRef ref;  // declared first after ctx: released after every buffer below
     int64_t n_nodes = 0, n_elem = 0;
     geo::DevBuf<double> xyz;       // SoA [3][N]
     geo::DevBuf<int32_t> conn;     // SoA [10][E]
@@ -45,6 +73,7 @@ struct geo_mesh {
 
 struct geo_dofs {
     geo_ctx* ctx = nullptr;
+    geo::CtxRef ref;  // declared first after ctx: released after every buffer below
     int64_t n_nodes = 0, n_dofs = 0, n_dir = 0;
     int dpn = 1;
     geo::DevBuf<uint8_t> mask;
@@ -53,6 +82,7 @@ struct geo_dofs {
 
 struct geo_csr {
     geo_ctx* ctx = nullptr;
+    geo::CtxRef ref;  // declared first after ctx: released after every buffer below
     int64_t n_rows = 0, n_cols = 0, nnz = 0;
     geo::DevBuf<int64_t> indptr;
     geo::DevBuf<int32_t> indices;

@@ -93,8 +93,12 @@ def test_c2_connectivity_element_matrices_and_csr_at_size(orc, geo):
     assert np.abs(fb - fb_o).max() <= RTOL * np.abs(fb_o).max()
 
 
-def _perturbed_states(op, u_full, r0, coef, e, h, Ke_e, dofs_e, dir_mask, solver):
-    """State differences d+- = u(coef_e e^{+-h}) - u by residual correction (module doc)."""
+def _perturbed_states(op, u_full, r0, coef, e, h, Ke_e, dofs_e, dir_mask, solver, bnorm):
+    """State differences d+- = u(coef_e e^{+-h}) - u by residual correction (module doc).
+    The correction's right-hand side is tiny; it is solved scaled to the forward
+    right-hand side's norm bnorm (the system is linear), so that the CG's absolute
+    thresholds (breakdown at |p.Ap| < 1e-30, iterative.rs:85) see the magnitudes
+    of a forward solve."""
     out = []
     for sgn in (1.0, -1.0):
         c = coef.copy()
@@ -103,9 +107,10 @@ def _perturbed_states(op, u_full, r0, coef, e, h, Ke_e, dofs_e, dir_mask, solver
         r = r0.copy()
         r[dofs_e] -= np.expm1(sgn * h) * (Ke_e @ u_full[dofs_e])
         r[dir_mask == 1] = 0.0
-        d, st = op.solve(r, solver)
-        assert st.converged
-        out.append(d)
+        sc = bnorm / np.linalg.norm(r)
+        d, st = op.solve(r * sc, solver)
+        assert st.converged, st
+        out.append(d / sc)
     op.set_coefficients(coef)
     return out
 
@@ -141,11 +146,12 @@ def test_c4_adjoint_gradient_vs_central_differences_at_size(orc, geo):
     grad, sa = op.vjp(dJ, u=u, solver=mixed)
     assert sa.converged
     u_full = np.where(mask == 1, vals, u)
-    r0 = op.lift_rhs(f) - op.apply(u_full)
+    fb = op.lift_rhs(f)
+    r0 = fb - op.apply(u_full)
     h = 1e-6
     for e in choice_distinct(2004, E, 20):
         Ke_e = orc.thermal_stiffness(xyz[conn[e]], k[e])
-        dp, dmn = _perturbed_states(op, u_full, r0, k, e, h, Ke_e, conn[e], mask, fp64)
+        dp, dmn = _perturbed_states(op, u_full, r0, k, e, h, Ke_e, conn[e], mask, fp64, np.linalg.norm(fb))
         fd = _fd(dp, dmn, u, that, obs, h)
         assert abs(grad[e] - fd) <= 1e-5 * abs(fd), (int(e), grad[e], fd)
 
@@ -185,12 +191,13 @@ def test_c5_elasticity_adjoint_gradient_vs_central_differences_at_size(orc, geo)
     grad, sa = op.vjp(dJ, u=u, solver=mixed)
     assert sa.converged
     u_full = np.where(mask == 1, vals, u)
-    r0 = op.lift_rhs(f) - op.apply(u_full)
+    fb = op.lift_rhs(f)
+    r0 = fb - op.apply(u_full)
     h = 1e-6
     for e in choice_distinct(3004, E, 10):
         Ke_e = orc.elasticity_stiffness(xyz[conn[e]], Ee[e], 0.25)
         dofs = (3 * conn[e][:, None] + np.arange(3)).ravel()
-        dp, dmn = _perturbed_states(op, u_full, r0, Ee, e, h, Ke_e, dofs, mask, fp64)
+        dp, dmn = _perturbed_states(op, u_full, r0, Ee, e, h, Ke_e, dofs, mask, fp64, np.linalg.norm(fb))
         fd = _fd(dp, dmn, u, uhat, obs, h)
         assert abs(grad[e] - fd) <= 1e-5 * abs(fd), (int(e), grad[e], fd)
 
