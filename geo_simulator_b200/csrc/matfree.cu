@@ -638,6 +638,9 @@ int setup_patch_kernels(geo_op* op, int slot) {
 // so that both can be compared and tested. Returns the kernel's grid (0: not used).
 template <int NBUF, int HG>
 int setup_t32_nbuf(geo_op* op, size_t smem) {
+    cudaFuncAttributes fa{};
+    GEO_CUDA(cudaFuncGetAttributes(&fa, k_patch_t32<NBUF, HG>));
+    if (smem + fa.sharedSizeBytes > kSmemLimit) return 0;
     GEO_CUDA(cudaFuncSetAttribute(k_patch_t32<NBUF, HG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_patch_t32<NBUF, HG>, kPatchBS, smem));
