@@ -812,6 +812,94 @@ def validate_extrapolation(n=48, nz=32, sample_iters=5, tol=1e-8):
             "full_cg_s": st.solve_time, "extrapolated_s": est, "ratio": est / st.solve_time, "cpu": model}
 
 
+# FP64 Jacobi-PCG iterations of the 48x48x24 elasticity system (rel-res 1e-8),
+# measured on a B200 by this repository's FP64 solver (same loop and rule); the CPU
+# table scales its sampled CG by it.
+ELASTICITY_FP64_ITERS = 838
+
+
+def cpu_table():
+    """The reference's path restated by the oracle on this host, per configuration:
+    assemble_*_stiffness_parallel (OpenMP element loop, serial triplet merge and
+    to_csr), the load, apply_dirichlet_bcs (serial) and the serial Jacobi-CG (full
+    solves for the thermal configurations; set-up + 5 iterations scaled by the
+    iteration count for elasticity). For the results table of the baseline."""
+    from geo_simulator_b200.fields import lognormal_field
+    from oracle import oracle as orc
+    L = orc.lib()
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
+    u8 = lambda a: a.ctypes.data_as(C.POINTER(C.c_uint8))
+
+    def cg(h, b, its, tol):
+        x = np.empty(b.size)
+        st = orc.OrcStats()
+        L.orc_cg_solve(h, dp(b), its, tol, 1e-12 if its > 0 else 0.0, 1, dp(x), C.byref(st))
+        return st
+
+    model, cores = host_cpu()
+    out = {"cpu": model, "host_cores": cores, "rows": []}
+    for name, dims, field, tol in (("C1 6x6x6 thermal, k = 3", (6, 6, 6), None, 1e-10),
+                                   ("C2 64x64x64 thermal, k = 3", (64, 64, 64), None, 1e-8),
+                                   ("C4 48x48x32 thermal, ln k ~ N(ln 3, 0.3^2)", (48, 48, 32), (2001, 0.3), 1e-8)):
+        xyz, conn = orc.generate_cube(*dims, LX, LY, LZ)
+        xyz, conn = np.ascontiguousarray(xyz), np.ascontiguousarray(conn, dtype=np.int64)
+        mask, vals = orc.thermal_bc(xyz, LZ)
+        mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        N, E = xyz.shape[0], conn.shape[0]
+        ke = None if field is None else lognormal_field(field[0], E, np.log(3.0), field[1])
+        t0 = time.perf_counter()
+        hk = L.orc_assemble_thermal_stiffness(N, dp(xyz), E, ip(conn), None if ke is None else dp(ke), 3.0, 1)
+        t1 = time.perf_counter()
+        f = np.empty(N)
+        L.orc_assemble_thermal_load(N, dp(xyz), E, ip(conn), Q, dp(f))
+        t2 = time.perf_counter()
+        fb = np.empty(N)
+        hb = L.orc_apply_dirichlet_bcs(hk, dp(f), u8(mask), dp(vals), dp(fb))
+        t3 = time.perf_counter()
+        st = cg(hb, fb, 100000, tol)
+        out["rows"].append({"config": name, "dofs": N, "nnz_K": L.orc_csr_nnz(hk), "nnz_Kbc": L.orc_csr_nnz(hb),
+                            "stiffness_s": t1 - t0, "load_s": t2 - t1, "dirichlet_s": t3 - t2, "rel_res": tol,
+                            "cg_s": st.solve_time, "cg_iterations": st.iterations, "cg_kind": "full solve"})
+        L.orc_csr_free(hk)
+        L.orc_csr_free(hb)
+    # C5 elasticity
+    lx, ly, lz = 100e3, 100e3, 50e3
+    xyz, conn = orc.generate_cube(48, 48, 24, lx, ly, lz)
+    xyz, conn = np.ascontiguousarray(xyz), np.ascontiguousarray(conn, dtype=np.int64)
+    N, E = xyz.shape[0], conn.shape[0]
+    x, y, z = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+    mask = np.zeros(3 * N, np.uint8)
+    base = np.nonzero(np.abs(z) < 1.0)[0]
+    for c in range(3):
+        mask[3 * base + c] = 1
+    mask[3 * np.nonzero((np.abs(x) < 1.0) | (np.abs(x - lx) < 1.0))[0]] = 1
+    mask[3 * np.nonzero((np.abs(y) < 1.0) | (np.abs(y - ly) < 1.0))[0] + 1] = 1
+    vals = np.zeros(3 * N)
+    Ee = lognormal_field(3001, E, np.log(1e11), 0.3)
+    t0 = time.perf_counter()
+    hk = L.orc_assemble_elasticity_stiffness(N, dp(xyz), E, ip(conn), dp(Ee), 0.0, 0.25, 1)
+    t1 = time.perf_counter()
+    f = np.empty(3 * N)
+    g = np.array([0.0, 0.0, -9.81])
+    L.orc_assemble_gravity_load(N, dp(xyz), E, ip(conn), 3300.0, dp(g), dp(f))
+    t2 = time.perf_counter()
+    fb = np.empty(3 * N)
+    hb = L.orc_apply_dirichlet_bcs(hk, dp(f), u8(mask), dp(vals), dp(fb))
+    t3 = time.perf_counter()
+    s0, s5 = cg(hb, fb, 0, 1e-30), cg(hb, fb, 5, 1e-30)
+    per = (s5.solve_time - s0.solve_time) / 5
+    out["rows"].append({"config": "C5 48x48x24 elasticity, ln E ~ N(ln 1e11, 0.3^2)", "dofs": 3 * N,
+                        "nnz_K": L.orc_csr_nnz(hk), "nnz_Kbc": L.orc_csr_nnz(hb), "stiffness_s": t1 - t0,
+                        "load_s": t2 - t1, "dirichlet_s": t3 - t2, "rel_res": 1e-8,
+                        "cg_s": s0.solve_time + per * (ELASTICITY_FP64_ITERS + 1),
+                        "cg_iterations": ELASTICITY_FP64_ITERS,
+                        "cg_kind": f"set-up {s0.solve_time:.2f} s + {per:.3f} s/iteration x the FP64 count"})
+    L.orc_csr_free(hk)
+    L.orc_csr_free(hb)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -828,6 +916,8 @@ def main():
                     help="also time Neumann, the Maxwell step, mesh generation and VTU output")
     ap.add_argument("--validate-extrapolation", action="store_true",
                     help="reference arm: one full CPU CG at 48x48x32 against its scaled sample")
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="reference arm: the oracle's assembly, Dirichlet and CG times at C1, C2, C4, C5")
     args = ap.parse_args()
     ws, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
@@ -835,6 +925,9 @@ def main():
             return
         if args.validate_extrapolation:
             print(json.dumps(validate_extrapolation()), flush=True)
+            return
+        if args.cpu_table:
+            print(json.dumps(cpu_table()), flush=True)
             return
         if (args.size, args.tol) not in FP64_ITERS:
             print(json.dumps({"impl": "reference",

@@ -11,7 +11,9 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libgeofem.so")
+# GEO_LIBRARY may name another build of the same library (same ABI), e.g. one
+# compiled with different launch bounds, to compare builds in one environment.
+LIB_PATH = os.environ.get("GEO_LIBRARY") or os.path.join(_HERE, "libgeofem.so")
 
 GEO_OK = 0
 GEO_ERR_INVALID_ARG = 1

@@ -20,7 +20,6 @@
 #include <cub/cub.cuh>
 
 #include "mf_kernels.cuh"
-#include "mf_thermal32.cuh"
 #include "pcg_common.cuh"
 
 struct geo_op;
@@ -474,10 +473,6 @@ struct geo_op {
     int nbuf[2] = {2, 2};              // element-data buffers of the patch kernel (FP64, FP32)
     int own_bulk[2] = {0, 0};          // own-node slices by bulk copy (FP32 thermal PCG), see setup
     size_t patch_smem[2] = {0, 0};     // dynamic shared memory of the patch kernel
-    // FP32 thermal PCG launches by k_patch_t32 (affine elements, halo mode, own-node
-    // slices): its grid and dynamic shared memory; t32 = 0 keeps k_patch
-    int t32 = 0, t32_grid = 0;
-    size_t t32_smem = 0;
     int node_grid[2] = {0, 0};  // resident node-kernel blocks (FP64, mixed)
     // CUDA graphs of PCG iteration chunks, keyed by precision
     cudaGraphExec_t chunk[2] = {nullptr, nullptr};
@@ -632,60 +627,8 @@ int setup_patch_kernels(geo_op* op, int slot) {
     return per_sm * op->ctx->sm_count;
 }
 
-// k_patch_t32 for the FP32 thermal PCG of affine meshes, when the operator runs the
-// PCG in halo mode with own-node slices by bulk copy (its shared-memory layout
-// holds in the general kernel's budget). GEO_PATCH_KERNEL=generic keeps k_patch,
-// so that both can be compared and tested. Returns the kernel's grid (0: not used).
-template <int NBUF, int HG>
-int setup_t32_nbuf(geo_op* op, size_t smem) {
-    cudaFuncAttributes fa{};
-    GEO_CUDA(cudaFuncGetAttributes(&fa, k_patch_t32<NBUF, HG>));
-    if (smem + fa.sharedSizeBytes > kSmemLimit) return 0;
-    GEO_CUDA(cudaFuncSetAttribute(k_patch_t32<NBUF, HG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    GEO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_patch_t32<NBUF, HG>, kPatchBS, smem));
-    return per_sm * op->ctx->sm_count;
-}
-
-void setup_t32(geo_op* op) {
-    op->t32 = 0;
-    const char* force = std::getenv("GEO_PATCH_KERNEL");
-    if (force && std::string(force) == "generic") return;
-    if (op->phys != 0 || op->nq != 1 || !op->own_bulk[1] || !op->halo[1]) return;
-    using K = ThermalK<float, 1>;
-    const int hm = op->halo[1] == 1 ? 1 : 0;
-    const size_t fixed = op->nbuf[1] == 2 ? patch_smem_tables<K, float, 2>(op->max_for, hm)
-                                          : patch_smem_tables<K, float, 1>(op->max_for, hm);
-    const size_t smem = fixed + t32_tables_bytes(op->max_local, op->max_own);
-    if (smem > kSmemLimit) return;
-    const bool hg = op->halo[1] == 2;
-    const int grid = op->nbuf[1] == 2 ? (hg ? setup_t32_nbuf<2, 1>(op, smem) : setup_t32_nbuf<2, 0>(op, smem))
-                                      : (hg ? setup_t32_nbuf<1, 1>(op, smem) : setup_t32_nbuf<1, 0>(op, smem));
-    if (grid < 1) return;
-    op->t32 = 1;
-    op->t32_grid = grid;
-    op->t32_smem = smem;
-}
-
 template <class K, class T, int MODE>
 void launch_patch(const geo_op* op, int slot, cudaStream_t s, const T* qd, const PatchArgs<T>& pa) {
-    if constexpr (std::is_same_v<K, ThermalK<float, 1>> && MODE == MODE_PCG) {
-        if (op->t32) {
-            const unsigned g = (unsigned)std::min(op->t32_grid, op->n_patches);
-            PatchView v = view(op);
-            v.own_bulk = 1;
-            v.halo = op->halo[1];
-            const size_t smem = op->t32_smem;
-            if (op->nbuf[1] == 2) {
-                if (v.halo == 2) k_patch_t32<2, 1><<<g, kPatchBS, smem, s>>>(v, qd, pa);
-                else k_patch_t32<2, 0><<<g, kPatchBS, smem, s>>>(v, qd, pa);
-            } else {
-                if (v.halo == 2) k_patch_t32<1, 1><<<g, kPatchBS, smem, s>>>(v, qd, pa);
-                else k_patch_t32<1, 0><<<g, kPatchBS, smem, s>>>(v, qd, pa);
-            }
-            return;
-        }
-    }
     const unsigned g = (unsigned)std::min(op->patch_grid[slot], op->n_patches);
     PatchView v = view(op);
     v.own_bulk = op->own_bulk[slot];
@@ -922,7 +865,6 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
         using K32 = decltype(k32);
         op->patch_grid[0] = setup_patch_kernels<K64, double>(op.get(), 0);
         op->patch_grid[1] = setup_patch_kernels<K32, float>(op.get(), 1);
-        setup_t32(op.get());
     });
     with_kernels(op.get(), [&](auto k64, auto k32) {
         int per_sm = 0;
@@ -944,8 +886,7 @@ geo_op* create_op(geo_ctx* ctx, const geo_mesh* mesh, const geo_dofs* dofs, int 
     op->bvec.alloc(op->ndof);
     op->xvec.alloc(op->ndof);
     op->state.alloc(1);
-    op->part.alloc((size_t)2 * std::max({op->patch_grid[0], op->patch_grid[1], op->node_grid[0], op->node_grid[1],
-                                         op->t32_grid}));
+    op->part.alloc((size_t)2 * std::max({op->patch_grid[0], op->patch_grid[1], op->node_grid[0], op->node_grid[1]}));
     GEO_CUDA(cudaMemset(op->state.p, 0, sizeof(PcgState)));
     GEO_CUDA(cudaMallocHost(&op->h_state, sizeof(PcgState)));
     return op.release();

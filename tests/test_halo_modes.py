@@ -1,7 +1,6 @@
 """The three ways the PCG's patch kernel hands shared-node contributions
 to the node update: red.global.add (mode 0), halo slots carried in shared memory
-(1) and halo slots read from global memory (2), for both FP32 thermal PCG patch
-kernels. The operator set-up picks one
+(1) and halo slots read from global memory (2). The operator set-up picks one
 by occupancy (2 only on large meshes); GEO_PATCH_HALO forces each here, and the
 solutions must agree with the oracle's CG and with each other, in FP64 and mixed
 precision. The node counts are not multiples of the node update's vector width,
@@ -15,13 +14,8 @@ from conftest import thermal_problem
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel", ["", "generic"])
 @pytest.mark.parametrize("n", [7, 12])
-def test_halo_modes_agree(orc, geo, n, kernel, monkeypatch):
-    """kernel "" lets the set-up pick k_patch_t32 for the FP32 thermal PCG (halo modes
-    1 and 2, affine mesh: patches start at every offset mod 4, the last one short);
-    "generic" keeps k_patch for it."""
-    monkeypatch.setenv("GEO_PATCH_KERNEL", kernel)
+def test_halo_modes_agree(orc, geo, n, monkeypatch):
     xyz, conn, mask, vals = thermal_problem(n, orc)
     rng = np.random.default_rng(n)
     k_e = np.exp(np.log(3.0) + 0.5 * rng.normal(size=conn.shape[0]))
