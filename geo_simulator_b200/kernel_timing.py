@@ -1,7 +1,7 @@
 """Per-kernel device times of one matrix-free PCG iteration on the thermal cube.
 
     python -m geo_simulator_b200.kernel_timing [--size 96] [--iterations 20]
-        [--precision mixed|fp64] [--physics thermal|elasticity]
+        [--nz NZ] [--precision mixed|fp64] [--physics thermal|elasticity]
     python -m geo_simulator_b200.kernel_timing --meshgen --size 128
     python -m geo_simulator_b200.kernel_timing --vtu --size 128 [--vtu-file PATH]
     python -m geo_simulator_b200.kernel_timing --csr --size 64 [--reps 2]
@@ -138,10 +138,10 @@ def vtu_timing(n, path=None):
     return out
 
 
-def build(size, physics):
+def build(size, physics, nz=None):
     import geo_simulator_b200 as geo
     from geo_simulator_b200.fields import lognormal_field
-    mesh = geo.ImprovedMeshGenerator.generate_cube(size, size, size, LX, LY, LZ)
+    mesh = geo.ImprovedMeshGenerator.generate_cube(size, size, nz or size, LX, LY, LZ)
     E, N = mesh.num_elements(), mesh.num_nodes()
     xyz = mesh.nodes
     if physics == "thermal":
@@ -201,6 +201,7 @@ def csr_timing(n, reps):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--size", type=int, default=96)
+    ap.add_argument("--nz", type=int, default=None, help="hexes along z (default: --size)")
     ap.add_argument("--iterations", type=int, default=20)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--physics", default="thermal", choices=["thermal", "elasticity"])
@@ -225,7 +226,7 @@ def main():
         print(json.dumps({"size": n, "nodes": dm.num_nodes(), "elements": dm.num_elements(),
                           "bytes": meshgen_bytes(dm.num_nodes(), dm.num_elements(), nv)}))
         return
-    mesh, op, fb = build(args.size, args.physics)
+    mesh, op, fb = build(args.size, args.physics, args.nz)
     prec = N.PRECISION_MIXED if args.precision == "mixed" else N.PRECISION_FP64
     pms, ums = C.c_double(), C.c_double()
     op.ctx.check(N.lib().geo_op_time_pcg_kernels(op.h, fb.ctypes.data, prec, args.iterations,
@@ -235,7 +236,7 @@ def main():
     dpn = 1 if args.physics == "thermal" else 3
     pb, ub = patch_pcg_bytes(E, Nn, s, dpn), update_bytes(Nn, s, dpn)
     print(json.dumps({
-        "size": args.size, "physics": args.physics, "precision": args.precision, "elements": E, "nodes": Nn,
+        "size": args.size, "nz": args.nz or args.size, "physics": args.physics, "precision": args.precision, "elements": E, "nodes": Nn,
         "iterations": args.iterations,
         "patch_ms": pms.value, "patch_bytes": pb, "patch_gbs": pb / pms.value / 1e6,
         "update_ms": ums.value, "update_bytes": ub, "update_gbs": ub / ums.value / 1e6,
