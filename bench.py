@@ -128,7 +128,7 @@ def solve_bytes(E, N, iters, nupd):
     """Algorithmic bytes of one mixed solve: per FP32 PCG iteration one patch-kernel
     and one node-update launch; per FP64 refresh one FP64 apply (E(20 + 48) + 2 N 8
     + N/8) plus 4 FP64 node streams."""
-    return (iters * (patch_pcg_bytes(E, N, 4) + update_bytes(N, 4))
+    return (iters * (patch_pcg_bytes(E, N, 4, zform=True) + update_bytes(N, 4, zform=True))
             + nupd * (E * (20 + 48) + 2 * N * 8 + N / 8 + 4 * N * 8))
 
 
@@ -403,8 +403,8 @@ def run_ours(args, ws, rank, local, pg):
                                               C.byref(pms), C.byref(ums)))
     patch_s, update_s = pms.value / 1e3, ums.value / 1e3
     hbm, peak_kind = peaks()
-    pbytes = patch_pcg_bytes(E, Nn, 4)
-    ubytes = update_bytes(Nn, 4)
+    pbytes = patch_pcg_bytes(E, Nn, 4, zform=True)
+    ubytes = update_bytes(Nn, 4, zform=True)
     achieved = pbytes / patch_s / 1e9
     traffic = (PATCH_PCG_F32_DRAM_BYTES_PER_ELEMENT * E) if PATCH_PCG_F32_DRAM_BYTES_PER_ELEMENT else None
     abytes = solve_bytes(E, Nn, iters, nupd)
@@ -427,13 +427,13 @@ def run_ours(args, ws, rank, local, pg):
         "traffic": traffic, "peak_kind": peak_kind,
         "kernel": "k_patch<ThermalK<float,1>, float, MODE_PCG> (FP32 PCG-mode patch kernel)",
         "algorithmic_bytes_per_launch": pbytes, "launch_s": patch_s,
-        "bytes_model": "E(20 + 6*4) + 5 N 4 + N/8: 16-bit local connectivity and G per element; "
-                       "r, D^-1, p_old read and p, q written per DOF; Dirichlet bitmask",
+        "bytes_model": "E(20 + 6*4) + 6 N 4 + N/8: 16-bit local connectivity and G per element; "
+                       "z, p_old, x read and p, q, x written per DOF; Dirichlet bitmask",
         "plain_apply_bytes": survey_apply_bytes(E, Nn, 4),
         "flops_per_launch": pflops, "tflops": pflops / patch_s / 1e12,
         "fp32_peak_tflops": cuda_core_peak_tflops(sm_mhz),
         "timing": f"CUDA events between launches, {kt_iters} PCG iterations after the timed region",
-        "node_update": {"kernel": "k_pcg_update_halo<float>", "launch_s": update_s,
+        "node_update": {"kernel": "k_pcg_update_halo<float, 1, true> (z-form)", "launch_s": update_s,
                         "algorithmic_bytes_per_launch": ubytes, "frac": ubytes / update_s / 1e9 / hbm},
         "solve": {"algorithmic_bytes": abytes, "device_s": kern, "frac": abytes / kern / 1e9 / hbm},
     }

@@ -173,6 +173,7 @@ struct PatchArgs {
     double* part;  // [gridDim.x][2]
     int* err;      // DEV_ERR_* bits (bounded waits)
     T* halo;       // halo mode: foreign contributions by slot (DPN values each)
+    T* xsol;       // PCG z-form: the FP32 solution correction, updated on the own nodes
 };
 
 // ------------------------------------------------------------------ bulk copy + mbarrier
@@ -312,12 +313,20 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     T* own_r = own_d + OCAP;
     T* own_p = own_r + OCAP;
     uint8_t* own_f = reinterpret_cast<uint8_t*>(own_p + OCAP);
-    T beta = T(0);
+    // Preconditioned-residual form of the mixed thermal PCG (FP32, one DOF per node):
+    // the node update keeps z = D^-1 r (a.r holds z) instead of r, so the gather
+    // forms p = z + beta p_old from two vectors, and the solution update
+    // x += alpha_prev p_old of the previous iteration rides here, on the own nodes'
+    // p_old (a.xsol holds the FP32 solution). The FP64 drop-in and elasticity keep the
+    // reference's form (iterative.rs:46-119).
+    constexpr bool ZF = MODE == MODE_PCG && std::is_same<T, float>::value && DPN == 1;
+    T beta = T(0), alpha_prev = T(0);
     const T* pold = nullptr;
     T* pnew = nullptr;
     if (MODE == MODE_PCG) {
         if (a.st->flags & (ST_DONE | ST_REFRESH)) return;
         beta = (T)a.st->beta;
+        if (ZF) alpha_prev = (T)a.st->alpha;
         const bool odd = a.st->it & 1;
         pold = odd ? a.pbuf1 : a.pbuf0;
         pnew = odd ? a.pbuf0 : a.pbuf1;
@@ -363,10 +372,10 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         const int f0 = o0 & ~15, nf = ((o1 + 15) & ~15) - f0;                             // flags, 16-byte aligned
         const uint32_t vb = (uint32_t)nv * (uint32_t)sizeof(T);
         mbar_expect_tx(&bar[2], 3u * vb + (uint32_t)nf);
-        if (nv) {
-            bulk_g2s(own_d, a.dinv + a0, vb, &bar[2]);
-            bulk_g2s(own_r, a.r + a0, vb, &bar[2]);
-            bulk_g2s(own_p, pold + a0, vb, &bar[2]);
+        if (nv) {  // z-form: z, p_old, x in the three slices; else D^-1, r, p_old
+            bulk_g2s(own_d, ZF ? a.r + a0 : a.dinv + a0, vb, &bar[2]);
+            bulk_g2s(own_r, ZF ? pold + a0 : a.r + a0, vb, &bar[2]);
+            bulk_g2s(own_p, ZF ? a.xsol + a0 : pold + a0, vb, &bar[2]);
         }
         if (nf) bulk_g2s(own_f, pv.flags + f0, (uint32_t)nf, &bar[2]);
     };
@@ -449,7 +458,11 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
 #pragma unroll
                     for (int c = 0; c < DPN; ++c) {
                         const int64_t idx = (int64_t)node[g] * DPN + c;
-                        if (MODE == MODE_PCG) {
+                        if (ZF) {
+                            d0[g][c] = a.r[idx];
+                            d1[g][c] = pold[idx];
+                            d2[g][c] = u < nown ? a.xsol[idx] : T(0);
+                        } else if (MODE == MODE_PCG) {
                             d0[g][c] = a.dinv[idx];
                             d1[g][c] = a.r[idx];
                             d2[g][c] = pold[idx];
@@ -469,9 +482,10 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                     const bool dir = (fl[g] >> c) & 1;
                     T v;
                     if (MODE == MODE_PCG) {
-                        const T pn = d0[g][c] * d1[g][c] + beta * d2[g][c];
+                        const T pn = ZF ? d0[g][c] + beta * d1[g][c] : d0[g][c] * d1[g][c] + beta * d2[g][c];
                         if (u < nown) {
                             pnew[(int64_t)node[g] * DPN + c] = pn;
+                            if (ZF) a.xsol[(int64_t)node[g] * DPN + c] = d2[g][c] + alpha_prev * d1[g][c];
                             if (dir) pdd += (double)(pn * pn);
                         }
                         v = dir ? T(0) : pn;
@@ -602,6 +616,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                 st->pAp = pAp;
                 if (fabs(pAp) < 1e-30) {  // iterative.rs:85
                     st->flags |= ST_DONE | ST_BREAKDOWN;
+                    st->alpha = 0.0;  // no step: the z-form's pending x update adds nothing
                 } else {
                     st->alpha = st->rz / pAp;
                 }
@@ -692,12 +707,21 @@ __device__ __forceinline__ void pcg_update_finish(const NodeArgs<T>& a, T acc_rr
 }
 
 // k_pcg_update_halo: one 16-byte vector per array in flight per thread, four
-// resident blocks (64 registers). The halo loads wait on the slot scan, so warps
+// resident blocks (64 registers; the z-form: six, below). The halo loads wait on the slot scan, so warps
 // hide that latency better than deeper unrolling: at 128^3 (FP32) 0.095 ms
 // against 0.107 ms (two vectors) and 0.20 ms (four, one block per SM).
+// The z-form update of the mixed thermal solver streams four vectors instead of
+// seven and fits six blocks per SM (42 registers): 0.073 ms at 128^3 against
+// 0.085 ms at four blocks and 0.081 ms at eight.
 constexpr int kHaloUnroll = 1;
 constexpr int kHaloMinBlocks = 4;
+constexpr int kHaloMinBlocksZ = 6;
 constexpr int kHaloShift = 3;  // flag bits 3-6: halo slots of the node (halo mode)
+
+// ro / dj for the norms of the z-form (FP32: the fast reciprocal-multiply, within
+// two units in the last place; the stopping and refresh tests do not need more)
+__device__ __forceinline__ float fast_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fast_div(double a, double b) { return a / b; }
 
 // Sum of node j's halo slots, starting at slot s (fixed order: slot order).
 template <class T>
@@ -714,7 +738,7 @@ __device__ __forceinline__ T halo_sum(const T* __restrict__ halo, int64_t s, int
 // hbase[first / 32] and each lane's first slot follows from a warp scan of the
 // lanes' slot counts. Loop conditions are warp-uniform (lanes past the end load
 // nothing and count 0 slots).
-template <class T, int kU>
+template <class T, int kU, bool ZF>
 __device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T cd, const T* __restrict__ p,
                                                 T& acc_rr, T& acc_rz) {
     using VT = typename Vec16<T>::type;
@@ -728,8 +752,18 @@ __device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T
     const int lane = threadIdx.x & 31;
     const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    // ZF (mixed thermal z-form, see k_patch): r holds z = D^-1 r, x is not touched
+    // (the next patch kernel updates it) and p is read only where a Dirichlet row needs it
     auto entry = [&](T pj, T qj, T xj, T rj, T dj, uint8_t f, T& xo, T& ro) {
         const T qq = (f & 1) ? cd * pj : qj;
+        if (ZF) {
+            ro = rj - alpha * (dj * qq);
+            const T rr = fast_div(ro, dj);
+            acc_rr += rr * rr;
+            acc_rz += rr * ro;
+            xo = xj;
+            return;
+        }
         xo = xj + alpha * pj;
         ro = rj - alpha * qq;
         acc_rr += ro * ro;
@@ -749,18 +783,22 @@ __device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T
     const int64_t nv = a.vec ? n / V : 0;
     int64_t iv = tid;
     for (; iv - lane + 31 + (kU - 1) * nth < nv; iv += kU * nth) {  // all lanes, all u in range
-        VT pv[kU], qv[kU], xv[kU], rv[kU], dv[kU];
+        VT pv[kU] = {}, qv[kU], xv[kU], rv[kU], dv[kU];
         uint8_t fl[kU][V];
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
             const int64_t k = iv + u * nth;
-            pv[u] = reinterpret_cast<const VT*>(p)[k];
             qv[u] = reinterpret_cast<const VT*>(q)[k];
-            xv[u] = reinterpret_cast<const VT*>(x)[k];
+            if (!ZF) xv[u] = reinterpret_cast<const VT*>(x)[k];
             rv[u] = reinterpret_cast<const VT*>(r)[k];
             dv[u] = reinterpret_cast<const VT*>(dinv)[k];
+            uint8_t any_dir = 0;
 #pragma unroll
-            for (int e = 0; e < V; ++e) fl[u][e] = flags[k * V + e];
+            for (int e = 0; e < V; ++e) {
+                fl[u][e] = flags[k * V + e];
+                any_dir |= fl[u][e];
+            }
+            if (!ZF || (any_dir & 1)) pv[u] = reinterpret_cast<const VT*>(p)[k];
         }
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
@@ -786,7 +824,7 @@ __device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T
                 sl += cnt[e];
                 entry(pe[e], qj, xe[e], re[e], de[e], fl[u][e], xoe[e], roe[e]);
             }
-            reinterpret_cast<VT*>(x)[k] = xo;
+            if (!ZF) reinterpret_cast<VT*>(x)[k] = xo;
             reinterpret_cast<VT*>(r)[k] = ro;
         }
     }
@@ -803,7 +841,7 @@ __device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T
         int64_t sl = lane_slot(iv, tot);
         if (in) {
             const VT pv = reinterpret_cast<const VT*>(p)[iv], qv = reinterpret_cast<const VT*>(q)[iv];
-            const VT xv = reinterpret_cast<const VT*>(x)[iv], rv = reinterpret_cast<const VT*>(r)[iv];
+            const VT xv = ZF ? VT{} : reinterpret_cast<const VT*>(x)[iv], rv = reinterpret_cast<const VT*>(r)[iv];
             const VT dv = reinterpret_cast<const VT*>(dinv)[iv];
             VT xo, ro;
 #pragma unroll
@@ -814,7 +852,7 @@ __device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T
                       reinterpret_cast<const T*>(&rv)[e], reinterpret_cast<const T*>(&dv)[e], fl[e],
                       reinterpret_cast<T*>(&xo)[e], reinterpret_cast<T*>(&ro)[e]);
             }
-            reinterpret_cast<VT*>(x)[iv] = xo;
+            if (!ZF) reinterpret_cast<VT*>(x)[iv] = xo;
             reinterpret_cast<VT*>(r)[iv] = ro;
         }
     }
@@ -825,8 +863,8 @@ __device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T
         int64_t sl = a.hbase[j / 32];
         for (int64_t i = j & ~(int64_t)31; i < j; ++i) sl += (flags[i] >> kHaloShift) & 15;
         T xo, ro;
-        entry(p[j], q[j] + halo_sum(halo, sl, (f >> kHaloShift) & 15), x[j], r[j], dinv[j], f, xo, ro);
-        x[j] = xo;
+        entry(p[j], q[j] + halo_sum(halo, sl, (f >> kHaloShift) & 15), ZF ? T(0) : x[j], r[j], dinv[j], f, xo, ro);
+        if (!ZF) x[j] = xo;
         r[j] = ro;
     }
 }
@@ -848,12 +886,23 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
     const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     T acc_rr = T(0), acc_rz = T(0);
-    // one entry: new x and r, q zeroed where another patch accumulates into it next time
+    // z-form (mixed thermal, see k_patch): r holds z = D^-1 r and x is updated by the
+    // next patch kernel
+    constexpr bool ZF = MIXED && DPN == 1 && std::is_same<T, float>::value;
+    // one entry: new x and r (z-form: new z), q zeroed where another patch accumulates into it next time
     auto entry = [&](int64_t j, T pj, T qj, T xj, T rj, T dj, T& xo, T& ro) {
         const uint8_t f = flags[j / DPN];
         const bool dir = (f >> (j % DPN)) & 1;
         const T qq = dir ? cd * pj : qj;
         if (!dir && (f & kFlagShared)) q[j] = T(0);
+        if (ZF) {
+            ro = rj - alpha * (dj * qq);
+            const T rr = fast_div(ro, dj);
+            acc_rr += rr * rr;
+            acc_rz += rr * ro;
+            xo = xj;
+            return;
+        }
         xo = xj + alpha * pj;
         ro = rj - alpha * qq;
         acc_rr += ro * ro;
@@ -868,7 +917,7 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
             const int64_t k = iv + u * nth;
             pv[u] = reinterpret_cast<const VT*>(p)[k];
             qv[u] = reinterpret_cast<const VT*>(q)[k];
-            xv[u] = reinterpret_cast<const VT*>(x)[k];
+            if (!ZF) xv[u] = reinterpret_cast<const VT*>(x)[k];
             rv[u] = reinterpret_cast<const VT*>(r)[k];
             dv[u] = reinterpret_cast<const VT*>(dinv)[k];
         }
@@ -885,13 +934,13 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
             T* roe = reinterpret_cast<T*>(&ro);
 #pragma unroll
             for (int e = 0; e < V; ++e) entry(k * V + e, pe[e], qe[e], xe[e], re[e], de[e], xoe[e], roe[e]);
-            reinterpret_cast<VT*>(x)[k] = xo;
+            if (!ZF) reinterpret_cast<VT*>(x)[k] = xo;
             reinterpret_cast<VT*>(r)[k] = ro;
         }
     }
     for (; iv < nv; iv += nth) {
         const VT pv = reinterpret_cast<const VT*>(p)[iv], qv = reinterpret_cast<const VT*>(q)[iv];
-        const VT xv = reinterpret_cast<const VT*>(x)[iv], rv = reinterpret_cast<const VT*>(r)[iv];
+        const VT xv = ZF ? VT{} : reinterpret_cast<const VT*>(x)[iv], rv = reinterpret_cast<const VT*>(r)[iv];
         const VT dv = reinterpret_cast<const VT*>(dinv)[iv];
         VT xo, ro;
 #pragma unroll
@@ -899,13 +948,13 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
             entry(iv * V + e, reinterpret_cast<const T*>(&pv)[e], reinterpret_cast<const T*>(&qv)[e],
                   reinterpret_cast<const T*>(&xv)[e], reinterpret_cast<const T*>(&rv)[e],
                   reinterpret_cast<const T*>(&dv)[e], reinterpret_cast<T*>(&xo)[e], reinterpret_cast<T*>(&ro)[e]);
-        reinterpret_cast<VT*>(x)[iv] = xo;
+        if (!ZF) reinterpret_cast<VT*>(x)[iv] = xo;
         reinterpret_cast<VT*>(r)[iv] = ro;
     }
     for (int64_t j = nv * V + tid; j < n; j += nth) {
         T xo, ro;
-        entry(j, p[j], q[j], x[j], r[j], dinv[j], xo, ro);
-        x[j] = xo;
+        entry(j, p[j], q[j], ZF ? T(0) : x[j], r[j], dinv[j], xo, ro);
+        if (!ZF) x[j] = xo;
         r[j] = ro;
     }
     pcg_update_finish<T, MIXED>(a, acc_rr, acc_rz);
@@ -1053,12 +1102,16 @@ __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, 
 
 // Node update of a PCG in halo mode (see pcg_update_halo / pcg_update_halo3).
 template <class T, int DPN, bool MIXED>
-__global__ void __launch_bounds__(kNodeBS, kHaloMinBlocks) k_pcg_update_halo(NodeArgs<T> a) {
+__global__ void __launch_bounds__(kNodeBS, (MIXED && DPN == 1 && std::is_same<T, float>::value) ? kHaloMinBlocksZ
+                                                                                             : kHaloMinBlocks)
+    k_pcg_update_halo(NodeArgs<T> a) {
     PcgState* st = a.st;
     if (st->flags & (ST_DONE | ST_REFRESH)) return;
     const T* __restrict__ p = (st->it & 1) ? a.pbuf0 : a.pbuf1;
     T acc_rr = T(0), acc_rz = T(0);
-    if (DPN == 1) pcg_update_halo<T, kHaloUnroll>(a, (T)st->alpha, (T)st->cd, p, acc_rr, acc_rz);
+    if (DPN == 1)
+        pcg_update_halo<T, kHaloUnroll, MIXED && std::is_same<T, float>::value>(a, (T)st->alpha, (T)st->cd, p,
+                                                                                 acc_rr, acc_rz);
     else pcg_update_halo3<T>(a, (T)st->alpha, (T)st->cd, p, acc_rr, acc_rz);
     pcg_update_finish<T, MIXED>(a, acc_rr, acc_rz);
 }
@@ -1145,10 +1198,12 @@ __global__ void __launch_bounds__(kNodeBS) k_mixed_init2(NodeArgs<float> a) {
     const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
     const double inv = 1.0 / a.st->s_scale;
     double rz = 0.0;
+    const bool zf = a.dpn == 1;  // mixed thermal keeps z = D^-1 r (see k_patch)
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += nth) {
         const float ri = (float)(a.b[i] * inv);
-        a.r[i] = ri;
-        rz += (double)(ri * (ri * a.dinv[i]));
+        const float zi = ri * a.dinv[i];
+        a.r[i] = zf ? zi : ri;
+        rz += (double)(ri * zi);
     }
     double v[1] = {rz};
     store_partial<1>(a.part, v);
@@ -1162,11 +1217,18 @@ __global__ void __launch_bounds__(kNodeBS) k_mixed_init2(NodeArgs<float> a) {
     }
 }
 
-// MIXED refresh 1: x64 += s xs, xs = 0.
+// MIXED refresh 1: x64 += s xs, xs = 0. In the z-form (one DOF per node) xs still
+// lacks the last step alpha p of the iteration that asked for the refresh (the next
+// patch kernel would have added it): it is added here, and k_refresh_residual sets
+// alpha to 0 so that no later patch kernel adds it again.
 __global__ void __launch_bounds__(kNodeBS) k_refresh_flush(NodeArgs<float> a) {
     const double s = a.st->s_scale;
+    const bool zf = a.dpn == 1;
+    const float alpha = zf ? (float)a.st->alpha : 0.0f;
+    const float* p = (a.st->it & 1) ? a.pbuf1 : a.pbuf0;  // the last direction
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
-        a.x64[i] += s * (double)a.x[i];
+        const float xi = zf ? a.x[i] + alpha * p[i] : a.x[i];
+        a.x64[i] += s * (double)xi;
         a.x[i] = 0.0f;
     }
 }
@@ -1192,6 +1254,7 @@ __global__ void __launch_bounds__(kNodeBS) k_refresh_residual(NodeArgs<float> a)
         if (threadIdx.x == 0) {
             st->ticket[TICKET_AUX] = 0;
             const double s_new = sqrt(t[0]);
+            st->alpha = 0.0;  // the last step is in x64 now (k_refresh_flush)
             st->nupd += 1;
             st->res = s_new;
             st->s_new = s_new;
@@ -1257,6 +1320,7 @@ __global__ void __launch_bounds__(kNodeBS) k_refresh_residual_halo(NodeArgs<floa
         if (threadIdx.x == 0) {
             st->ticket[TICKET_AUX] = 0;
             const double s_new = sqrt(t[0]);
+            st->alpha = 0.0;  // the last step is in x64 now (k_refresh_flush)
             st->nupd += 1;
             st->res = s_new;
             st->s_new = s_new;
@@ -1307,6 +1371,7 @@ __global__ void __launch_bounds__(kNodeBS) k_refresh_rescale(NodeArgs<float> a) 
     if (st->flags & ST_DONE) return;
     const double inv = 1.0 / st->s_new;
     const float ratio = (float)st->ratio;
+    const bool zf = a.dpn == 1;  // z-form: r holds z = D^-1 r
     float* p = (st->it & 1) ? a.pbuf1 : a.pbuf0;  // direction the next apply reads
     double rz = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -1314,9 +1379,10 @@ __global__ void __launch_bounds__(kNodeBS) k_refresh_rescale(NodeArgs<float> a) 
         const double wi = a.w64[i];
         if (!((fl >> (i % a.dpn)) & 1) && (fl & kFlagShared)) a.w64[i] = 0.0;
         const float ri = (float)(wi * inv);
-        a.r[i] = ri;
+        const float zi = ri * a.dinv[i];
+        a.r[i] = zf ? zi : ri;
         p[i] *= ratio;
-        rz += (double)(ri * (ri * a.dinv[i]));
+        rz += (double)(ri * zi);
     }
     double v[1] = {rz};
     store_partial<1>(a.part, v);

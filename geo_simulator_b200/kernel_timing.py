@@ -44,19 +44,21 @@ LX, LY, LZ = 1000.0, 1000.0, 600.0
 NQD = {1: 6, 3: 10}
 
 
-def patch_pcg_bytes(E, N, s, dpn=1):
+def patch_pcg_bytes(E, N, s, dpn=1, zform=False):
     """Bytes one PCG-mode patch-kernel launch must move: per element its paired
     16-bit patch-local connectivity (20 B) and its qdata (6 or 10 values of s
-    bytes); per DOF r, D^-1 and the previous p read, the new p and q = K p written;
-    the Dirichlet bitmask. (The node coordinates are not read: the operator stores
-    qdata instead.)"""
-    return E * (20 + NQD[dpn] * s) + N * dpn * 5 * s + N / 8
+    bytes); per DOF r, D^-1 and the previous p read, the new p and q = K p written
+    (zform, the mixed thermal solver: z and the previous p read, p and q written,
+    the solution read and written); the Dirichlet bitmask. (The node coordinates are
+    not read: the operator stores qdata instead.)"""
+    return E * (20 + NQD[dpn] * s) + N * dpn * (6 if zform else 5) * s + N / 8
 
 
-def update_bytes(N, s, dpn=1):
+def update_bytes(N, s, dpn=1, zform=False):
     """Algorithmic bytes of one node-update launch: p, q, x, r, D^-1 read, x and r
-    written, Dirichlet bitmask."""
-    return N * dpn * 7 * s + N * dpn / 8
+    written, Dirichlet bitmask (zform: q, z, D^-1 read, z written; p only on
+    Dirichlet rows)."""
+    return N * dpn * (4 if zform else 7) * s + N * dpn / 8
 
 
 # Floating-point operations per element of one PCG-mode patch-kernel launch,
@@ -234,7 +236,8 @@ def main():
     E, Nn = mesh.num_elements(), mesh.num_nodes()
     s = 4 if args.precision == "mixed" else 8
     dpn = 1 if args.physics == "thermal" else 3
-    pb, ub = patch_pcg_bytes(E, Nn, s, dpn), update_bytes(Nn, s, dpn)
+    zf = args.precision == "mixed" and dpn == 1  # the mixed thermal solver runs the z-form
+    pb, ub = patch_pcg_bytes(E, Nn, s, dpn, zf), update_bytes(Nn, s, dpn, zf)
     print(json.dumps({
         "size": args.size, "nz": args.nz or args.size, "physics": args.physics, "precision": args.precision, "elements": E, "nodes": Nn,
         "iterations": args.iterations,
