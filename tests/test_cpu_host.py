@@ -107,7 +107,7 @@ def test_bench_byte_and_flop_model():
     assert kt.patch_pcg_bytes(E, N, 4, zform=True) == pytest.approx(E * 44 + N * 24 + N / 8)
     assert kt.update_bytes(N, 4, zform=True) == pytest.approx(16 * N + N / 8)
     assert bench.solve_bytes(E, N, 10, 1) == pytest.approx(
-        10 * (kt.patch_pcg_bytes(E, N, 4, True) + kt.update_bytes(N, 4, zform=True)) + E * 68 + 16 * N + N / 8
+        10 * (kt.patch_pcg_bytes(E, N, 4, zform=True) + kt.update_bytes(N, 4, zform=True)) + E * 68 + 16 * N + N / 8
         + 32 * N)
     # FLOPs per element from the kernels' formulation; CUDA-core peaks at 1965 MHz
     assert kt.patch_pcg_flops(E, N) == E * 216 + 3 * N
