@@ -642,6 +642,53 @@ def elasticity_config(ctx, clk=None):
             "patch_kernels": kern}
 
 
+def gpu_table(ctx):
+    """GPU side of the baseline's results table for the configurations the bench
+    line does not cover: C1 (6^3, k = 3, rel-res 1e-10: CSR assembly + Dirichlet,
+    the FP64 CSR PCG drop-in, the FP64 and mixed matrix-free solves) and C4
+    (48x48x32, ln k ~ N(ln 3, 0.3^2): FP64 and mixed matrix-free forward solves to
+    rel-res 1e-8). Device time by CUDA events on the context stream."""
+    import geo_simulator_b200 as geo
+    from geo_simulator_b200.fields import lognormal_field
+    out = {}
+    mesh, _, mask, vals = thermal_inputs(6)
+    dm = geo.DofManager(mesh.num_nodes(), 1)
+    idx = np.nonzero(mask)[0]
+    dm.set_dirichlet(idx, vals[idx])
+    f = geo.Assembler.assemble_thermal_load(mesh, dm, Q, ctx)
+    cg = lambda t: geo.ConjugateGradient().with_tolerance(t).with_max_iterations(20000)
+    asm = lambda: geo.Assembler.apply_dirichlet_bcs(geo.Assembler.assemble_thermal_stiffness_parallel(
+        mesh, dm, 3.0, ctx), f, dm, ctx)
+    asm()
+    t_asm, (Kb, fb) = _device_timed(ctx, asm, 5)
+    cg(1e-10).solve(Kb, fb)
+    t_csr, (_, st_csr) = _device_timed(ctx, lambda: cg(1e-10).solve(Kb, fb), 5)
+    op = geo.ThermalOperator(mesh, dm, 3.0, ctx)
+    op.solve(fb, cg(1e-10))
+    t_mf, (_, st_mf) = _device_timed(ctx, lambda: op.solve(fb, cg(1e-10)), 5)
+    mixed = cg(1e-10).with_precision("mixed")
+    op.solve(fb, mixed)
+    t_mx, (_, st_mx) = _device_timed(ctx, lambda: op.solve(fb, mixed), 5)
+    out["C1"] = {"csr_assembly_and_bc_s": t_asm, "csr_pcg_s": t_csr, "csr_iterations": st_csr.iterations,
+                 "matfree_fp64_s": t_mf, "matfree_fp64_iterations": st_mf.iterations,
+                 "mixed_s": t_mx, "mixed_iterations": st_mx.iterations, "rel_res": 1e-10}
+    mesh, _, mask, vals = thermal_inputs(48, nz=32)
+    k_e = lognormal_field(2001, mesh.num_elements(), np.log(3.0), 0.3)
+    dm = geo.DofManager(mesh.num_nodes(), 1)
+    idx = np.nonzero(mask)[0]
+    dm.set_dirichlet(idx, vals[idx])
+    op = geo.ThermalOperator(mesh, dm, k_e, ctx)
+    f = geo.Assembler.assemble_thermal_load(mesh, dm, Q, ctx)
+    row = {"rel_res": NOMINAL_TOL}
+    for name, solver in (("fp64", cg(NOMINAL_TOL)), ("mixed", cg(NOMINAL_TOL).with_precision("mixed"))):
+        op.forward(f, solver)
+        t, (_, st) = _device_timed(ctx, lambda: op.forward(f, solver), 3)
+        row[f"{name}_forward_s"] = t
+        row[f"{name}_iterations"] = st.iterations
+    out["C4"] = row
+    return out
+
+
 def neumann_timing(ctx, mesh):
     """Neumann flux on the top face of the 128^3 cube: GPU boundary-face detection
     (find_boundary_faces) and the deterministic apply_neumann_bcs, host-timed."""
@@ -918,6 +965,8 @@ def main():
                     help="reference arm: one full CPU CG at 48x48x32 against its scaled sample")
     ap.add_argument("--cpu-table", action="store_true",
                     help="reference arm: the oracle's assembly, Dirichlet and CG times at C1, C2, C4, C5")
+    ap.add_argument("--gpu-table", action="store_true",
+                    help="our arm: GPU times at C1 and C4 for the baseline's results table, then exit")
     args = ap.parse_args()
     ws, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
@@ -934,6 +983,10 @@ def main():
                               "unavailable": f"no FP64 iteration count known for size {args.size}, tol {args.tol:g}"}))
             return
         print(json.dumps(run_reference(args)), flush=True)
+        return
+    if args.gpu_table:
+        import geo_simulator_b200 as geo
+        print(json.dumps(gpu_table(geo.Context(local))), flush=True)
         return
     line = run_ours(args, ws, rank, local, pg)
     if rank == 0:
