@@ -581,10 +581,7 @@ int setup_patch_nbuf(size_t attr_bytes, size_t plain, size_t own, int& per_sm_pl
 // nodes, which was slower than the plain gather (80^3, 112^3). Returns the grid.
 template <class K, class T>
 int setup_patch_kernels(geo_op* op, int slot) {
-#ifndef PATCH64_NBUF
-#define PATCH64_NBUF 2
-#endif
-    int nbuf = (std::is_same<T, double>::value && K::DPN == 1) ? PATCH64_NBUF : 2;
+    int nbuf = 2;
     if (smem_bytes<K, T>(op, 2, false) > kSmemLimit) {
         if (smem_bytes<K, T>(op, 1, false) > kSmemLimit)
             fail(GEO_ERR_UNSUPPORTED, "patch tables exceed shared memory (too many nodes per patch)");

@@ -287,11 +287,8 @@ __host__ __device__ inline size_t patch_smem_tables(int max_for, int halo) {
 
 // HG = 1: the halo-mode variant whose flush reads the halo slots from global
 // memory (PatchView::halo == 2); HG = 0 serves every other launch.
-#ifndef PATCH64_MINB
-#define PATCH64_MINB 1
-#endif
 template <class K, class T, int MODE, int NBUF, int HG = 0>
-__global__ void __launch_bounds__(kPatchBS, (std::is_same<T, double>::value && K::DPN == 1) ? PATCH64_MINB : 1) k_patch(PatchView pv, const T* __restrict__ qd_all, T cl, T cm,
+__global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __restrict__ qd_all, T cl, T cm,
                                                     PatchArgs<T> a) {
     constexpr int DPN = K::DPN;
     constexpr uint32_t LCB = patch_bytes_lc<K, T>(), QDB = patch_bytes_qd<K, T>();
