@@ -220,7 +220,7 @@ __global__ void k_halo_flags(const int32_t* __restrict__ cnt, int64_t N, uint8_t
 }
 
 // Largest number of a patch's elements that touch one patch-local node. One
-// block per patch; counts in shared memory (max_local ints).
+// block per patch; counts in shared memory (max_local ints, by slot).
 __global__ void k_patch_maxinc(const int32_t* __restrict__ pe, const int32_t* __restrict__ po,
                                const int32_t* __restrict__ pf, const uint32_t* __restrict__ lc, int32_t* maxinc) {
     extern __shared__ int cnt[];
@@ -228,18 +228,19 @@ __global__ void k_patch_maxinc(const int32_t* __restrict__ pe, const int32_t* __
     const int p = blockIdx.x;
     const int n_el = pe[p + 1] - pe[p];
     const int nloc = (po[p + 1] - po[p]) + (pf[p + 1] - pf[p]);
-    for (int u = threadIdx.x; u < nloc; u += blockDim.x) cnt[u] = 0;
+    const int nslot = nloc > 0 ? patch_slot(nloc - 1) + 1 : 0;  // lc holds slots
+    for (int u = threadIdx.x; u < nslot; u += blockDim.x) cnt[u] = 0;
     if (threadIdx.x == 0) s_max = 0;
     __syncthreads();
     for (int t = threadIdx.x; t < n_el * 10; t += blockDim.x) {
         const int j = t / 10, l = t % 10;
         const uint32_t w = lc[((int64_t)p * 5 + l / 2) * kPatchElems + j];
         const int u = (int)((l & 1) ? (w >> 16) : (w & 0xffffu));
-        if (u < nloc) atomicAdd(&cnt[u], 1);
+        if (u < nslot) atomicAdd(&cnt[u], 1);
     }
     __syncthreads();
     int m = 0;
-    for (int u = threadIdx.x; u < nloc; u += blockDim.x) m = max(m, cnt[u]);
+    for (int u = threadIdx.x; u < nslot; u += blockDim.x) m = max(m, cnt[u]);
     atomicMax(&s_max, m);
     __syncthreads();
     if (threadIdx.x == 0) maxinc[p] = s_max;

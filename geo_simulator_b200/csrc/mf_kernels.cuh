@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     unsigned char* ebuf = smem + 32;
     const bool OWNB = own_bulk<K, T, MODE>() && pv.own_bulk != 0;
     using SC = Scatter<T>;
-    const int M = pv.max_local * DPN;  // DOF slots of the patch-local table
+    const int M = pv.max_local * DPN;  // DOF slots of the patch-local table (nodes by patch_slot)
     unsigned char* abuf = smem + patch_smem_fixed<K, T, NBUF>();  // NBUF x (meta | ids | flags)
     const bool HALO = HG != 0 || pv.halo != 0;
     const int HMODE = !HALO ? 0 : (HG ? 2 : 1);  // 1: slots in shared memory, 2: from global
@@ -493,10 +493,10 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                         v = d0[g][c];
                         if (MODE == MODE_FREE ? dir : !dir) v = T(0);
                     }
-                    xs[u * DPN + c] = v;
+                    xs[patch_slot(u) * DPN + c] = v;
                     xlo[c] = fminf(xlo[c], (float)v);
                     xhi[c] = fmaxf(xhi[c], (float)v);
-                    SC::zero(ys, M, u * DPN + c);
+                    SC::zero(ys, M, patch_slot(u) * DPN + c);
                 }
             }
         }
@@ -573,7 +573,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             if (HALO) {  // own nodes stored, foreign ones to their halo slots (DPN values each)
                 if (DPN == 1) {  // kept apart: the general form costs the FP32 thermal kernel 9 registers
                     if (fl & 1) continue;
-                    const T v = SC::get(ys, M, u) * invS;
+                    const T v = SC::get(ys, M, patch_slot(u)) * invS;
                     if (u < nown) a.y[o0 + u] = v;
                     else a.halo[HG ? __ldg(pv.fslot + pm.fa + (u - nown)) : sfsl[u - nown]] = v;
                     continue;
@@ -583,7 +583,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                 T* dst = u < nown ? a.y : a.halo;
 #pragma unroll
                 for (int c = 0; c < DPN; ++c)
-                    if (!((fl >> c) & 1)) dst[base + c] = SC::get(ys, M, u * DPN + c) * invS;
+                    if (!((fl >> c) & 1)) dst[base + c] = SC::get(ys, M, patch_slot(u) * DPN + c) * invS;
                 continue;
             }
             const int node = u < nown ? o0 + u : sfor[u - nown];
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
 #pragma unroll
             for (int c = 0; c < DPN; ++c) {
                 if ((fl >> c) & 1) continue;
-                const T v = SC::get(ys, M, u * DPN + c) * invS;
+                const T v = SC::get(ys, M, patch_slot(u) * DPN + c) * invS;
                 T* dst = a.y + (int64_t)node * DPN + c;
                 if (plain) *dst = v;
                 else atomicAdd(dst, v);

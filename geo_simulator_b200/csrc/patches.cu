@@ -254,8 +254,9 @@ __global__ void k_local_conn(const int32_t* __restrict__ conn, const int32_t* __
         if (lo >= pf[p + 1] || foreign[lo] != nn) atomicOr(err, DEV_ERR_BOUNDS);
         loc = nown + (lo - pf[p]);
     }
-    if (loc > 65535) atomicOr(err, DEV_ERR_BOUNDS);
-    lconn[(int64_t)l * E + ne] = (uint16_t)loc;
+    const int64_t slot = loc + (loc >> 5);  // patch_slot
+    if (slot > 65535) atomicOr(err, DEV_ERR_BOUNDS);
+    lconn[(int64_t)l * E + ne] = (uint16_t)slot;
 }
 
 __global__ void k_local_sizes(const int32_t* po, const int32_t* pf, int P, int* out) {
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(32 * kOrderWarps)
 k_patch_order(const uint16_t* __restrict__ lconn, int64_t E, const int32_t* __restrict__ pe, int P,
               int32_t* __restrict__ wperm) {
     __shared__ uint16_t sl[kOrderWarps][10][kPatchElems];
-    __shared__ uint32_t used[kOrderWarps][10 * kPatchElems / 32];
+    __shared__ uint32_t used[kOrderWarps][(patch_slot(10 * kPatchElems) + 31) / 32];
     __shared__ uint8_t taken[kOrderWarps][kPatchElems];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = blockIdx.x * kOrderWarps + w;
@@ -429,7 +430,7 @@ void build_patches(cudaStream_t s, int64_t N, const double* xyz, int64_t E, cons
     GEO_CUDA(cudaMemcpyAsync(h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     GEO_CUDA(cudaStreamSynchronize(s));
     if (h[0]) fail(GEO_ERR_UNSUPPORTED, "patch-local index out of range while building the element patches");
-    L.max_local = h[1];
+    L.max_local = h[1] > 0 ? patch_slot(h[1] - 1) + 1 : 0;  // table size in slots
     // ---- conflict-avoiding element order inside each patch, patch-major connectivity
     {
         DevBuf<int32_t> wperm(E), eperm2(E);

@@ -17,6 +17,14 @@ namespace geo {
 
 constexpr int kPatchElems = 384;
 
+// Shared-memory slot of patch-local node u in the patch kernels' node tables:
+// one unused word after every 32 nodes. First-touch numbering places the nodes
+// that a warp's 32 elements read in one access at strides that share banks; the
+// padding spreads them (an emulation of the layout on a structured cube: 4.2 ->
+// 2.8 shared-memory wavefronts per warp access of the element phase). The 16-bit
+// local connectivity holds slots; loops over a patch's nodes map u -> slot.
+__host__ __device__ constexpr int patch_slot(int u) { return u + (u >> 5); }
+
 // node flag bits (patch numbering)
 constexpr uint8_t kFlagDir0 = 1;      // component c is Dirichlet: kFlagDir0 << c
 constexpr uint8_t kFlagShared = 128;  // touched by more than one patch
@@ -24,7 +32,7 @@ constexpr uint8_t kFlagShared = 128;  // touched by more than one patch
 struct PatchLayout {
     int64_t n_elem = 0, n_nodes = 0;
     int n_patches = 0;
-    int max_local = 0;          // largest patch-local node table
+    int max_local = 0;          // largest patch-local node table, in slots (patch_slot)
     DevBuf<int32_t> eperm;      // new element -> original element
     DevBuf<int32_t> nperm;      // new node -> original node
     DevBuf<int32_t> ninv;       // original node -> new node
@@ -34,7 +42,7 @@ struct PatchLayout {
     DevBuf<int32_t> foreign;        // new node ids, ascending per patch
     // Patch-major local connectivity, two 16-bit indices per word:
     // lc[(p * 5 + l / 2) * kPatchElems + j] holds, in bits 16*(l%2).., the
-    // patch-local node index of local node l of the patch's element j (entries
+    // slot (patch_slot) of local node l of the patch's element j (entries
     // past a short last patch are 0). Within a patch, elements are ordered so that
     // every aligned group of 32 (one warp) shares no node where possible.
     DevBuf<uint32_t> lc;            // [n_patches][5][kPatchElems]
