@@ -631,7 +631,7 @@ def elasticity_config(ctx, clk=None):
         pms, ums = C.c_double(), C.c_double()
         ctx.check(N.lib().geo_op_time_pcg_kernels(op.h, fb.ctypes.data, prec, 40, C.byref(pms), C.byref(ums)))
         fl = patch_pcg_flops(E, Nn, 3)
-        b = patch_pcg_bytes(E, Nn, 8 if fp64k else 4, 3)
+        b = patch_pcg_bytes(E, Nn, 8 if fp64k else 4, 3, zform=not fp64k)
         kern[name] = {"patch_ms": pms.value, "update_ms": ums.value, "tflops": fl / pms.value / 1e9,
                       "frac_cuda_core_peak": fl / pms.value / 1e9 / cuda_core_peak_tflops(sm_mhz, fp64k),
                       "gbs": b / pms.value / 1e6, "frac_hbm": b / pms.value / 1e6 / peaks()[0]}

@@ -1024,7 +1024,7 @@ PcgLaunchArgs pcg_args(geo_op* op, bool mixed) {
         p32.pbuf0 = n32.pbuf0;
         p32.pbuf1 = n32.pbuf1;
         p32.y = n32.q;
-        p32.xsol = n32.x;  // updated by the patch kernel in the z-form (one DOF per node)
+        p32.xsol = n32.x;  // updated by the patch kernel (z-form of the mixed solver)
     }
     if (op->halo[0]) {
         n64.halo = p64.halo = op->halo64.p;

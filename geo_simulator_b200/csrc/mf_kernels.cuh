@@ -313,13 +313,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     T* own_r = own_d + OCAP;
     T* own_p = own_r + OCAP;
     uint8_t* own_f = reinterpret_cast<uint8_t*>(own_p + OCAP);
-    // Preconditioned-residual form of the mixed thermal PCG (FP32, one DOF per node):
+    // Preconditioned-residual form of the mixed solver's FP32 PCG (thermal and elasticity):
     // the node update keeps z = D^-1 r (a.r holds z) instead of r, so the gather
     // forms p = z + beta p_old from two vectors, and the solution update
     // x += alpha_prev p_old of the previous iteration rides here, on the own nodes'
-    // p_old (a.xsol holds the FP32 solution). The FP64 drop-in and elasticity keep the
+    // p_old (a.xsol holds the FP32 solution). The FP64 drop-in keeps the
     // reference's form (iterative.rs:46-119).
-    constexpr bool ZF = MODE == MODE_PCG && std::is_same<T, float>::value && DPN == 1;
+    constexpr bool ZF = MODE == MODE_PCG && std::is_same<T, float>::value;
     T beta = T(0), alpha_prev = T(0);
     const T* pold = nullptr;
     T* pnew = nullptr;
@@ -752,7 +752,7 @@ __device__ __forceinline__ void pcg_update_halo(const NodeArgs<T>& a, T alpha, T
     const int lane = threadIdx.x & 31;
     const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    // ZF (mixed thermal z-form, see k_patch): r holds z = D^-1 r, x is not touched
+    // ZF (mixed solver's z-form, see k_patch): r holds z = D^-1 r, x is not touched
     // (the next patch kernel updates it) and p is read only where a Dirichlet row needs it
     auto entry = [&](T pj, T qj, T xj, T rj, T dj, uint8_t f, T& xo, T& ro) {
         const T qq = (f & 1) ? cd * pj : qj;
@@ -886,9 +886,9 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
     const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     T acc_rr = T(0), acc_rz = T(0);
-    // z-form (mixed thermal, see k_patch): r holds z = D^-1 r and x is updated by the
+    // z-form (the mixed solver, see k_patch): r holds z = D^-1 r and x is updated by the
     // next patch kernel
-    constexpr bool ZF = MIXED && DPN == 1 && std::is_same<T, float>::value;
+    constexpr bool ZF = MIXED && std::is_same<T, float>::value;
     // one entry: new x and r (z-form: new z), q zeroed where another patch accumulates into it next time
     auto entry = [&](int64_t j, T pj, T qj, T xj, T rj, T dj, T& xo, T& ro) {
         const uint8_t f = flags[j / DPN];
@@ -964,7 +964,7 @@ __global__ void __launch_bounds__(kNodeBS) k_pcg_update(NodeArgs<T> a) {
 // interleaved DOFs of every vector by scalar loads (issued before the slot scan),
 // then its slots' three components. A warp's 32 lanes are 32 consecutive nodes
 // starting at a multiple of 32, as in pcg_update_halo.
-template <class T>
+template <class T, bool ZF>
 __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, T cd, const T* __restrict__ p,
                                                  T& acc_rr, T& acc_rz) {
     const uint8_t* __restrict__ flags = a.flags;
@@ -989,11 +989,13 @@ __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, 
                 if (in) {
                     f[0] = flags[2 * m];
                     f[1] = flags[2 * m + 1];
+                    // z-form: p only where a Dirichlet row needs it, x not touched
+                    const bool need_p = !ZF || ((f[0] | f[1]) & 7);
     #pragma unroll
                     for (int k = 0; k < 3; ++k) {
-                        const float2 tp = reinterpret_cast<const float2*>(p)[3 * m + k];
+                        const float2 tp = need_p ? reinterpret_cast<const float2*>(p)[3 * m + k] : make_float2(0.f, 0.f);
                         const float2 tq = reinterpret_cast<const float2*>(q)[3 * m + k];
-                        const float2 tx = reinterpret_cast<const float2*>(x)[3 * m + k];
+                        const float2 tx = ZF ? make_float2(0.f, 0.f) : reinterpret_cast<const float2*>(x)[3 * m + k];
                         const float2 tr = reinterpret_cast<const float2*>(r)[3 * m + k];
                         const float2 td = reinterpret_cast<const float2*>(dinv)[3 * m + k];
                         pv[2 * k] = tp.x, pv[2 * k + 1] = tp.y;
@@ -1024,6 +1026,13 @@ __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, 
                         float h = 0.0f;
                         for (int i = 0; i < cnt; ++i) h += halo[3 * (se + i) + c];
                         const float qq = ((f[e] >> c) & 1) ? (float)cd * pv[v] : qv[v] + h;
+                        if (ZF) {  // rv holds z = D^-1 r
+                            rv[v] = rv[v] - (float)alpha * (dv[v] * qq);
+                            const float rr = fast_div(rv[v], dv[v]);
+                            acc_rr += rr * rr;
+                            acc_rz += rr * rv[v];
+                            continue;
+                        }
                         xv[v] = xv[v] + (float)alpha * pv[v];
                         rv[v] = rv[v] - (float)alpha * qq;
                         acc_rr += rv[v] * rv[v];
@@ -1032,7 +1041,7 @@ __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, 
                 }
     #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    reinterpret_cast<float2*>(x)[3 * m + k] = make_float2(xv[2 * k], xv[2 * k + 1]);
+                    if (!ZF) reinterpret_cast<float2*>(x)[3 * m + k] = make_float2(xv[2 * k], xv[2 * k + 1]);
                     reinterpret_cast<float2*>(r)[3 * m + k] = make_float2(rv[2 * k], rv[2 * k + 1]);
                 }
             }
@@ -1048,6 +1057,14 @@ __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, 
                     T h = T(0);
                     for (int i = 0; i < cnt; ++i) h += halo[3 * (s0 + i) + c];
                     const T qq = ((f >> c) & 1) ? cd * p[j] : q[j] + h;
+                    if (ZF) {
+                        const T zo = r[j] - alpha * (dinv[j] * qq);
+                        const T rr = fast_div(zo, dinv[j]);
+                        r[j] = zo;
+                        acc_rr += rr * rr;
+                        acc_rz += rr * zo;
+                        continue;
+                    }
                     const T xo = x[j] + alpha * p[j];
                     const T ro = r[j] - alpha * qq;
                     x[j] = xo;
@@ -1070,7 +1087,7 @@ __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, 
                 const int64_t j = 3 * nd + c;
                 pv[c] = p[j];
                 qv[c] = q[j];
-                xv[c] = x[j];
+                xv[c] = ZF ? T(0) : x[j];
                 rv[c] = r[j];
                 dv[c] = dinv[j];
             }
@@ -1090,6 +1107,14 @@ __device__ __forceinline__ void pcg_update_halo3(const NodeArgs<T>& a, T alpha, 
             T h = T(0);
             for (int i = 0; i < cnt; ++i) h += halo[3 * (s0 + i) + c];
             const T qq = ((f >> c) & 1) ? cd * pv[c] : qv[c] + h;
+            if (ZF) {
+                const T zo = rv[c] - alpha * (dv[c] * qq);
+                const T rr = fast_div(zo, dv[c]);
+                r[3 * nd + c] = zo;
+                acc_rr += rr * rr;
+                acc_rz += rr * zo;
+                continue;
+            }
             const T xo = xv[c] + alpha * pv[c];
             const T ro = rv[c] - alpha * qq;
             x[3 * nd + c] = xo;
@@ -1112,7 +1137,7 @@ __global__ void __launch_bounds__(kNodeBS, (MIXED && DPN == 1 && std::is_same<T,
     if (DPN == 1)
         pcg_update_halo<T, kHaloUnroll, MIXED && std::is_same<T, float>::value>(a, (T)st->alpha, (T)st->cd, p,
                                                                                  acc_rr, acc_rz);
-    else pcg_update_halo3<T>(a, (T)st->alpha, (T)st->cd, p, acc_rr, acc_rz);
+    else pcg_update_halo3<T, MIXED && std::is_same<T, float>::value>(a, (T)st->alpha, (T)st->cd, p, acc_rr, acc_rz);
     pcg_update_finish<T, MIXED>(a, acc_rr, acc_rz);
 }
 
@@ -1198,7 +1223,7 @@ __global__ void __launch_bounds__(kNodeBS) k_mixed_init2(NodeArgs<float> a) {
     const int64_t n = a.n, nth = (int64_t)gridDim.x * blockDim.x;
     const double inv = 1.0 / a.st->s_scale;
     double rz = 0.0;
-    const bool zf = a.dpn == 1;  // mixed thermal keeps z = D^-1 r (see k_patch)
+    const bool zf = true;  // the mixed solver keeps z = D^-1 r (see k_patch)
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += nth) {
         const float ri = (float)(a.b[i] * inv);
         const float zi = ri * a.dinv[i];
@@ -1217,13 +1242,13 @@ __global__ void __launch_bounds__(kNodeBS) k_mixed_init2(NodeArgs<float> a) {
     }
 }
 
-// MIXED refresh 1: x64 += s xs, xs = 0. In the z-form (one DOF per node) xs still
+// MIXED refresh 1: x64 += s xs, xs = 0. In the z-form xs still
 // lacks the last step alpha p of the iteration that asked for the refresh (the next
 // patch kernel would have added it): it is added here, and k_refresh_residual sets
 // alpha to 0 so that no later patch kernel adds it again.
 __global__ void __launch_bounds__(kNodeBS) k_refresh_flush(NodeArgs<float> a) {
     const double s = a.st->s_scale;
-    const bool zf = a.dpn == 1;
+    const bool zf = true;  // z-form (see k_patch)
     const float alpha = zf ? (float)a.st->alpha : 0.0f;
     const float* p = (a.st->it & 1) ? a.pbuf1 : a.pbuf0;  // the last direction
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -1371,7 +1396,7 @@ __global__ void __launch_bounds__(kNodeBS) k_refresh_rescale(NodeArgs<float> a) 
     if (st->flags & ST_DONE) return;
     const double inv = 1.0 / st->s_new;
     const float ratio = (float)st->ratio;
-    const bool zf = a.dpn == 1;  // z-form: r holds z = D^-1 r
+    const bool zf = true;  // z-form: r holds z = D^-1 r
     float* p = (st->it & 1) ? a.pbuf1 : a.pbuf0;  // direction the next apply reads
     double rz = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {

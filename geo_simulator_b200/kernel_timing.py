@@ -236,7 +236,7 @@ def main():
     E, Nn = mesh.num_elements(), mesh.num_nodes()
     s = 4 if args.precision == "mixed" else 8
     dpn = 1 if args.physics == "thermal" else 3
-    zf = args.precision == "mixed" and dpn == 1  # the mixed thermal solver runs the z-form
+    zf = args.precision == "mixed"  # the mixed solver runs the z-form
     pb, ub = patch_pcg_bytes(E, Nn, s, dpn, zf), update_bytes(Nn, s, dpn, zf)
     print(json.dumps({
         "size": args.size, "nz": args.nz or args.size, "physics": args.physics, "precision": args.precision, "elements": E, "nodes": Nn,
