@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cmath>
+#include <cstring>
 #include <type_traits>
 
 #include <cub/cub.cuh>
@@ -528,10 +529,11 @@ PatchView view(const geo_op* op) {
 // dynamic shared memory of the patch kernel: barriers, element-data buffers, node tables
 template <class K, class T>
 size_t smem_bytes(const geo_op* op, int nbuf, bool own, int halo = 0) {
-    // xs (T), fixed-point accumulators (Scatter<T>::kWords INT32 words), flags, and for
-    // FP32 thermal PCG the own-node slices
+    // xs (T), fixed-point accumulators (Scatter<T>::kWords INT32 words), flags (two
+    // tables in the late loop shape), and for PCG the own-node slices
+    const size_t flag_tables = nbuf == 2 ? patch_flag_tables<K, T, 2>() : patch_flag_tables<K, T, 1>();
     const size_t tables = (size_t)op->max_local * K::DPN * (sizeof(T) + 4 * Scatter<T>::kWords) +
-                          (size_t)op->max_local + 16 +
+                          (size_t)op->max_local * flag_tables + 16 +
                           (own ? (size_t)own_bytes<T>(op->max_own, K::DPN) : 0);
     return (nbuf == 2 ? patch_smem_tables<K, T, 2>(op->max_for, halo) : patch_smem_tables<K, T, 1>(op->max_for, halo)) +
            tables;
@@ -583,7 +585,9 @@ int setup_patch_nbuf(size_t attr_bytes, size_t plain, size_t own, int& per_sm_pl
 template <class K, class T>
 int setup_patch_kernels(geo_op* op, int slot) {
     int nbuf = 2;
-    if (smem_bytes<K, T>(op, 2, false) > kSmemLimit) {
+    // GEO_PATCH_NBUF=1 forces the single-buffer kernel, so that tests cover it on small meshes
+    const char* force_nbuf = std::getenv("GEO_PATCH_NBUF");
+    if (smem_bytes<K, T>(op, 2, false) > kSmemLimit || (force_nbuf && std::strcmp(force_nbuf, "1") == 0)) {
         if (smem_bytes<K, T>(op, 1, false) > kSmemLimit)
             fail(GEO_ERR_UNSUPPORTED, "patch tables exceed shared memory (too many nodes per patch)");
         nbuf = 1;

@@ -109,6 +109,12 @@ struct Scatter<float> {
         atomicAdd(acc + slot, __float2int_rn(v));
     }
     __device__ __forceinline__ static float get(const int* acc, int, int slot) { return (float)acc[slot]; }
+    // read and clear (the flush leaves the table zero for the next patch)
+    __device__ __forceinline__ static float take(int* acc, int, int slot) {
+        const int v = acc[slot];
+        acc[slot] = 0;
+        return (float)v;
+    }
 };
 
 template <>
@@ -132,6 +138,11 @@ struct Scatter<double> {
     }
     __device__ __forceinline__ static double get(const int* acc, int m, int slot) {
         return fma((double)acc[slot], 4398046511104.0, fma((double)acc[m + slot], 2097152.0, (double)acc[2 * m + slot]));
+    }
+    __device__ __forceinline__ static double take(int* acc, int m, int slot) {
+        const double v = get(acc, m, slot);
+        zero(acc, m, slot);
+        return v;
     }
 };
 
@@ -274,8 +285,25 @@ __host__ __device__ constexpr bool own_bulk() {
     return MODE == MODE_PCG;
 }
 
+// Loop shape of the double-buffered patch kernel.
+// - Early (FP32 thermal): the next patch's copy is issued at the top of the loop,
+//   a whole patch ahead, and a block barrier after the flush frees the buffer it
+//   overwrites. Its gather is short next to the copy's latency.
+// - Late (the others): the copy is issued after the gather barrier, when every warp
+//   has left the previous flush. No barrier follows the flush, so fast warps start
+//   the next gather while others still flush; the node flags then need one table
+//   per patch parity.
+template <class K, class T, int NBUF>
+__host__ __device__ constexpr bool patch_late() {
+    return NBUF == 2 && !(K::DPN == 1 && sizeof(T) == 4);
+}
+template <class K, class T, int NBUF>
+__host__ __device__ constexpr int patch_flag_tables() {
+    return patch_late<K, T, NBUF>() ? 2 : 1;
+}
+
 // shared memory layout: [3 mbarriers (32 B) | NBUF x (lc | qd) | NBUF x (meta | foreign ids | foreign flags) |
-// xs | ys | flags | own-node slices (FP32 thermal)]
+// xs | ys | flags (one table, two in the late shape) | own-node slices (PCG)]
 template <class K, class T, int NBUF>
 __host__ __device__ constexpr size_t patch_smem_fixed() {
     return 32 + (size_t)NBUF * (patch_bytes_lc<K, T>() + patch_bytes_qd<K, T>());
@@ -285,11 +313,21 @@ __host__ __device__ inline size_t patch_smem_tables(int max_for, int halo) {
     return patch_smem_fixed<K, T, NBUF>() + (size_t)NBUF * patch_aux_bytes(max_for, halo);
 }
 
+// Resident blocks per SM the register allocation must allow (the minimum-blocks
+// argument of the launch bounds): FP32 elasticity and FP64 thermal 2, FP64
+// elasticity 1, as many as their shared memory allows on the bench meshes. FP32
+// thermal gets no target (0): it compiles to 79-80 registers, 4 blocks of 192
+// threads, by itself, and a target of 4 made the same register count run 2% slower.
+template <class K, class T>
+__host__ __device__ constexpr int patch_min_blocks() {
+    return sizeof(T) == 4 ? (K::DPN == 1 ? 0 : 2) : (K::DPN == 1 ? 2 : 1);
+}
+
 // HG = 1: the halo-mode variant whose flush reads the halo slots from global
 // memory (PatchView::halo == 2); HG = 0 serves every other launch.
 template <class K, class T, int MODE, int NBUF, int HG = 0>
-__global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __restrict__ qd_all, T cl, T cm,
-                                                    PatchArgs<T> a) {
+__global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
+    k_patch(PatchView pv, const T* __restrict__ qd_all, T cl, T cm, PatchArgs<T> a) {
     constexpr int DPN = K::DPN;
     constexpr uint32_t LCB = patch_bytes_lc<K, T>(), QDB = patch_bytes_qd<K, T>();
     extern __shared__ __align__(128) unsigned char smem[];
@@ -307,9 +345,13 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     int* ys = reinterpret_cast<int*>(xs + M);  // fixed-point accumulators, SC::kWords x M words
     // FP32 scatter: per component, min and max of x over the patch as order keys, by patch parity
     __shared__ unsigned s_lo[2][DPN], s_hi[2][DPN];
-    uint8_t* sfl = reinterpret_cast<uint8_t*>(ys + SC::kWords * M);
+    constexpr bool LATE = patch_late<K, T, NBUF>();
+    // node flags; in the late shape by patch parity, since the flush of one patch
+    // reads them while faster warps already gather the next one
+    uint8_t* sfl0 = reinterpret_cast<uint8_t*>(ys + SC::kWords * M);
     const uint32_t OCAP = own_cap<T>(pv.max_own, DPN);
-    T* own_d = reinterpret_cast<T*>(smem + (((size_t)(sfl + pv.max_local - smem) + 15) & ~(size_t)15));
+    T* own_d = reinterpret_cast<T*>(
+        smem + (((size_t)(sfl0 + patch_flag_tables<K, T, NBUF>() * pv.max_local - smem) + 15) & ~(size_t)15));
     T* own_r = own_d + OCAP;
     T* own_p = own_r + OCAP;
     uint8_t* own_f = reinterpret_cast<uint8_t*>(own_p + OCAP);
@@ -340,6 +382,8 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             s_hi[0][c] = s_hi[1][c] = 0u;
         }
     }
+    // the accumulators start at zero; each flush clears what it reads
+    for (int i = threadIdx.x; i < SC::kWords * M; i += blockDim.x) ys[i] = 0;
     __syncthreads();
     // thread 0: the patch's element data, sizes, foreign ids and foreign flags into buffer b
     auto issue = [&](int patch, int b) {
@@ -390,11 +434,14 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
     int k = 0;
     for (int patch = blockIdx.x; patch < pv.n_patches; patch += gridDim.x, ++k) {
         const int b = NBUF == 2 ? (k & 1) : 0;
-        if (NBUF == 2 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) {
+        const bool has_next = patch + (int)gridDim.x < pv.n_patches;
+        if (!LATE && NBUF == 2 && threadIdx.x == 0 && has_next) {
             issue(patch + gridDim.x, b ^ 1);
             pend |= 1u << (b ^ 1);
         }
-        // the patch's sizes, element data and foreign lists (copied during the previous patch)
+        // The patch's sizes, element data and foreign lists. No block barrier here: a
+        // thread whose bounded wait ran out skips the gather, and the gather barrier
+        // below ends the block.
         bool ok = mbar_wait(&bar[b], (phase >> b) & 1);
         if (ok) {
             phase ^= 1u << b;
@@ -408,15 +455,7 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             }
             ok = ok && ok2;
         }
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) {
-                atomicOr(a.err, DEV_ERR_TIMEOUT);
-                // let copies still in flight land (bounded waits) before the block's shared memory is released
-                for (int q = 0; q < 3; ++q)
-                    if ((pend >> q) & 1) mbar_wait(&bar[q], (phase >> q) & 1);
-            }
-            return;
-        }
+        uint8_t* sfl = sfl0 + (LATE ? (k & 1) * pv.max_local : 0);
         const unsigned char* ab = abuf + (size_t)b * AUX;
         const PatchMeta pm = *reinterpret_cast<const PatchMeta*>(ab);
         const int* __restrict__ sfor = reinterpret_cast<const int*>(ab + sizeof(PatchMeta));
@@ -432,7 +471,8 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
         }
         // 1. gather (overlaps the bulk copies in flight); each thread issues the
         //    loads of up to kGather nodes before any store
-        for (int u0 = threadIdx.x; u0 < nloc; u0 += kGather * blockDim.x) {
+        const int nloc_g = ok ? nloc : 0;
+        for (int u0 = threadIdx.x; u0 < nloc_g; u0 += kGather * blockDim.x) {
             int node[kGather];
             uint8_t fl[kGather];
             T d0[kGather][DPN], d1[kGather][DPN], d2[kGather][DPN];
@@ -496,7 +536,6 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                     xs[patch_slot(u) * DPN + c] = v;
                     xlo[c] = fminf(xlo[c], (float)v);
                     xhi[c] = fmaxf(xhi[c], (float)v);
-                    SC::zero(ys, M, patch_slot(u) * DPN + c);
                 }
             }
         }
@@ -511,11 +550,27 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                 }
             }
         }
-        __syncthreads();
-        // the own-node buffer is free again: bring the next patch's slices during steps 2 and 3
-        if (OWNB && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) {
-            issue_own(patch + gridDim.x);
-            pend |= 4u;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicOr(a.err, DEV_ERR_TIMEOUT);
+                // let copies still in flight land (bounded waits) before the block's shared memory is released
+                for (int q = 0; q < 3; ++q)
+                    if ((pend >> q) & 1) mbar_wait(&bar[q], (phase >> q) & 1);
+            }
+            return;
+        }
+        // Every warp has left the previous patch's flush: in the late shape its buffer
+        // takes the next patch's copy; the own-node buffer (read by the gather only)
+        // takes the next patch's slices, during steps 2 and 3.
+        if (threadIdx.x == 0 && has_next) {
+            if (LATE) {
+                issue(patch + gridDim.x, b ^ 1);
+                pend |= 1u << (b ^ 1);
+            }
+            if (OWNB) {
+                issue_own(patch + gridDim.x);
+                pend |= 4u;
+            }
         }
         // 2. elements, scattered as fixed-point integers with scale S (see Scatter)
         T S = T(1), invS = T(1);
@@ -572,8 +627,8 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
             const uint8_t fl = sfl[u];
             if (HALO) {  // own nodes stored, foreign ones to their halo slots (DPN values each)
                 if (DPN == 1) {  // kept apart: the general form costs the FP32 thermal kernel 9 registers
+                    const T v = SC::take(ys, M, patch_slot(u)) * invS;
                     if (fl & 1) continue;
-                    const T v = SC::get(ys, M, patch_slot(u)) * invS;
                     if (u < nown) a.y[o0 + u] = v;
                     else a.halo[HG ? __ldg(pv.fslot + pm.fa + (u - nown)) : sfsl[u - nown]] = v;
                     continue;
@@ -582,25 +637,31 @@ __global__ void __launch_bounds__(kPatchBS) k_patch(PatchView pv, const T* __res
                                               : (int64_t)(HG ? __ldg(pv.fslot + pm.fa + (u - nown)) : sfsl[u - nown]) * DPN;
                 T* dst = u < nown ? a.y : a.halo;
 #pragma unroll
-                for (int c = 0; c < DPN; ++c)
-                    if (!((fl >> c) & 1)) dst[base + c] = SC::get(ys, M, patch_slot(u) * DPN + c) * invS;
+                for (int c = 0; c < DPN; ++c) {
+                    const T v = SC::take(ys, M, patch_slot(u) * DPN + c) * invS;
+                    if (!((fl >> c) & 1)) dst[base + c] = v;
+                }
                 continue;
             }
             const int node = u < nown ? o0 + u : sfor[u - nown];
             const bool plain = u < nown && !(fl & kFlagShared);
 #pragma unroll
             for (int c = 0; c < DPN; ++c) {
+                const T v = SC::take(ys, M, patch_slot(u) * DPN + c) * invS;
                 if ((fl >> c) & 1) continue;
-                const T v = SC::get(ys, M, patch_slot(u) * DPN + c) * invS;
                 T* dst = a.y + (int64_t)node * DPN + c;
                 if (plain) *dst = v;
                 else atomicAdd(dst, v);
             }
         }
-        __syncthreads();
-        if (NBUF == 1 && threadIdx.x == 0 && patch + (int)gridDim.x < pv.n_patches) {
-            issue(patch + gridDim.x, 0);
-            pend |= 1u;
+        // The late shape needs no barrier here: the next gather writes xs and the other
+        // flag table, which no flush reads, and the accumulators are zero again.
+        if (!LATE) {
+            __syncthreads();
+            if (NBUF == 1 && threadIdx.x == 0 && has_next) {
+                issue(patch + gridDim.x, 0);
+                pend |= 1u;
+            }
         }
     }
     if (MODE == MODE_PCG) {
