@@ -268,8 +268,12 @@ __global__ void k_local_sizes(const int32_t* po, const int32_t* pf, int P, int* 
 }
 
 // Orders each patch's elements so that every aligned group of 32 has pairwise
-// node-disjoint elements where possible (greedy), making the shared-memory
-// accumulation of a warp conflict-free. One warp per patch; lane 0 decides.
+// node-disjoint elements where possible (greedy in element order), making the
+// shared-memory accumulation of a warp conflict-free. One warp per patch. The
+// lanes test 32 consecutive candidates at once against the nodes the group
+// already uses; the lowest passing lane's element is the one a sequential scan
+// would take next, so it is taken, its nodes marked, and the lanes above it test
+// again. The result equals the sequential greedy's element for element.
 constexpr int kOrderWarps = 4;
 __global__ void __launch_bounds__(32 * kOrderWarps)
 k_patch_order(const uint16_t* __restrict__ lconn, int64_t E, const int32_t* __restrict__ pe, int P,
@@ -279,43 +283,67 @@ k_patch_order(const uint16_t* __restrict__ lconn, int64_t E, const int32_t* __re
     __shared__ uint8_t taken[kOrderWarps][kPatchElems];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = blockIdx.x * kOrderWarps + w;
-    if (p >= P) return;
+    if (p >= P) return;  // warp-uniform
     const int e0 = pe[p], n_el = pe[p + 1] - e0;
-    for (int t = lane; t < 10 * n_el; t += 32) sl[w][t / n_el][t % n_el] = lconn[(int64_t)(t / n_el) * E + e0 + t % n_el];
+    int nloc = 0;
+    for (int t = lane; t < 10 * n_el; t += 32) {
+        const uint16_t v = lconn[(int64_t)(t / n_el) * E + e0 + t % n_el];
+        sl[w][t / n_el][t % n_el] = v;
+        nloc = max(nloc, (int)v + 1);
+    }
+    nloc = __reduce_max_sync(0xffffffffu, nloc);
     for (int j = lane; j < n_el; j += 32) taken[w][j] = 0;
-    __syncwarp();
-    if (lane == 0) {
-        int nloc = 0;
-        for (int j = 0; j < n_el; ++j)
-            for (int l = 0; l < 10; ++l) nloc = max(nloc, (int)sl[w][l][j] + 1);
-        const int words = (nloc + 31) / 32;
-        int out = 0;
-        while (out < n_el) {
-            for (int k = 0; k < words; ++k) used[w][k] = 0u;
-            int cnt = 0;
-            for (int j = 0; j < n_el && cnt < 32; ++j) {
-                if (taken[w][j]) continue;
-                bool ok = true;
-                for (int l = 0; l < 10 && ok; ++l) {
-                    const int u = sl[w][l][j];
-                    ok = !((used[w][u >> 5] >> (u & 31)) & 1u);
+    const int words = (nloc + 31) / 32;
+    uint32_t* uw = used[w];
+    // element j (< n_el) shares no node with the group so far
+    auto disjoint = [&](int j) {
+        for (int l = 0; l < 10; ++l) {
+            const int u = sl[w][l][j];
+            if ((uw[u >> 5] >> (u & 31)) & 1u) return false;
+        }
+        return true;
+    };
+    int out = 0;  // warp-uniform
+    while (out < n_el) {
+        for (int k = lane; k < words; k += 32) uw[k] = 0u;
+        __syncwarp();
+        int cnt = 0;
+        for (int j0 = 0; j0 < n_el && cnt < 32; j0 += 32) {
+            const int j = j0 + lane;
+            bool cand = j < n_el && !taken[w][j] && disjoint(j);
+            unsigned m = __ballot_sync(0xffffffffu, cand);
+            while (m != 0u && cnt < 32) {
+                const int L = __ffs(m) - 1;
+                if (lane == L) {  // the only writer of the group's node bits
+                    for (int l = 0; l < 10; ++l) {
+                        const int u = sl[w][l][j];
+                        uw[u >> 5] |= 1u << (u & 31);
+                    }
+                    taken[w][j] = 1;
+                    wperm[e0 + out] = e0 + j;
                 }
-                if (!ok) continue;
-                for (int l = 0; l < 10; ++l) {
-                    const int u = sl[w][l][j];
-                    used[w][u >> 5] |= 1u << (u & 31);
+                ++out;
+                ++cnt;
+                __syncwarp();
+                cand = cand && lane > L && disjoint(j);
+                m = __ballot_sync(0xffffffffu, cand);
+            }
+        }
+        // keep groups aligned with warps: top up with the next untaken elements
+        for (int j0 = 0; j0 < n_el && cnt < 32 && out < n_el; j0 += 32) {
+            const int j = j0 + lane;
+            unsigned m = __ballot_sync(0xffffffffu, j < n_el && !taken[w][j]);
+            while (m != 0u && cnt < 32 && out < n_el) {
+                const int L = __ffs(m) - 1;
+                if (lane == L) {
+                    taken[w][j] = 1;
+                    wperm[e0 + out] = e0 + j;
                 }
-                taken[w][j] = 1;
-                wperm[e0 + out++] = e0 + j;
+                ++out;
                 ++cnt;
+                m &= m - 1u;
             }
-            // keep groups aligned with warps: top up with the next untaken elements
-            for (int j = 0; j < n_el && cnt < 32 && out < n_el; ++j) {
-                if (taken[w][j]) continue;
-                taken[w][j] = 1;
-                wperm[e0 + out++] = e0 + j;
-                ++cnt;
-            }
+            __syncwarp();
         }
     }
 }
