@@ -103,6 +103,7 @@ struct Scatter;
 template <>
 struct Scatter<float> {
     static constexpr float kLim = 1073741824.0f;  // 2^30
+    static constexpr int kLimExp = 30;
     static constexpr int kWords = 1;
     __device__ __forceinline__ static void zero(int* acc, int, int slot) { acc[slot] = 0; }
     __device__ __forceinline__ static void add(int* acc, int, int slot, float v) {
@@ -120,6 +121,7 @@ struct Scatter<float> {
 template <>
 struct Scatter<double> {
     static constexpr float kLim = 4.611686018427388e18f;  // 2^62
+    static constexpr int kLimExp = 62;
     static constexpr int kWords = 3;
     __device__ __forceinline__ static void zero(int* acc, int m, int slot) {
         acc[slot] = 0;
@@ -146,10 +148,19 @@ struct Scatter<double> {
     }
 };
 
-// power of two <= v (v > 0), clamped to [2^-100, 2^100]
-__device__ __forceinline__ float pow2_floor(float v) {
-    v = fminf(fmaxf(v, 7.888609e-31f), 1.2676506e30f);
-    return __uint_as_float(__float_as_uint(v) & 0x7f800000u);
+// S = the largest power of two <= 2^lim_exp / bx, clamped to [2^-100, 2^100], and
+// 1/S, both exact, from the exponent field of bx > 0 (no division): with
+// bx = m 2^e, m in [1, 2), S = 2^(lim_exp - e) when m = 1, else 2^(lim_exp - e - 1);
+// a subnormal bx gives the upper clamp, an infinite one the lower.
+__device__ __forceinline__ void pow2_scale(float bx, int lim_exp, float& S, float& invS) {
+    const unsigned bits = __float_as_uint(bx);
+    const int ef = (int)(bits >> 23);
+    int se = lim_exp - (ef - 127) - ((bits & 0x7fffffu) != 0u ? 1 : 0);
+    if (ef == 0) se = 100;
+    if (ef == 255) se = -100;
+    se = min(max(se, -100), 100);
+    S = __uint_as_float((unsigned)(se + 127) << 23);
+    invS = __uint_as_float((unsigned)(127 - se) << 23);
 }
 
 // float <-> unsigned key with the same order (for warp min/max reductions)
@@ -586,8 +597,10 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
             }
             const float bx = __fmul_ru(pbound, __fmaf_ru(mabs, 1.52587890625e-05f, half));  // 2^-16
             if (bx > 0.0f) {
-                S = (T)pow2_floor(SC::kLim / bx);
-                invS = T(1) / S;
+                float sf, isf;
+                pow2_scale(bx, SC::kLimExp, sf, isf);
+                S = (T)sf;
+                invS = (T)isf;
             }
             if (threadIdx.x < DPN) {  // next read by the patch after next
                 s_lo[(k + 1) & 1][threadIdx.x] = 0xffffffffu;
