@@ -459,6 +459,7 @@ struct geo_op {
     // per-patch bound of the fixed-point scatter (Scatter in mf_kernels.cuh)
     geo::DevBuf<int32_t> pmaxinc;
     geo::DevBuf<float> pbound32;
+    geo::DevBuf<geo::PatchMeta> prec;  // per-patch records (PatchView::rec)
     // solver workspace
     geo::DevBuf<double> w64;
     geo::DevBuf<float> w32;
@@ -523,6 +524,7 @@ PatchView view(const geo_op* op) {
     v.own_bulk = 0;
     v.fslot = op->fslot.p;
     v.halo = 0;
+    v.rec = op->prec.p;
     return v;
 }
 
@@ -734,6 +736,9 @@ void refresh_coefficients(geo_op* op) {
         k_patch_bound<<<(unsigned)cdiv(op->n_patches, 256), 256, 0, s>>>(op->pmaxinc.p, knorm, op->n_patches,
                                                                          op->pbound32.p);
         check_launch(ctx, "k_patch_bound");
+        op->prec.ensure(op->n_patches);
+        k_patch_records<<<(unsigned)cdiv(op->n_patches, 256), 256, 0, s>>>(view(op), op->prec.p);
+        check_launch(ctx, "k_patch_records");
         sync(ctx, "patch bounds");
     }
     op->ediag.ensure((size_t)op->E * 10 * op->dpn);

@@ -51,6 +51,8 @@ enum : int { MODE_FREE = 0, MODE_LIFT = 1, MODE_PCG = 2 };
 enum : int { ST_DONE = 1, ST_REFRESH = 2, ST_CONVERGED = 4, ST_BREAKDOWN = 8 };
 enum : int { TICKET_PATCH = 0, TICKET_UPDATE = 1, TICKET_AUX = 2 };
 
+struct PatchMeta;
+
 struct PatchView {
     int64_t E, N;
     int n_patches, max_local, dpn;
@@ -78,6 +80,10 @@ struct PatchView {
     // launches where the shared-memory copy would cost a resident block
     const int32_t* fslot;
     int halo;
+    // per patch: element count, own range, foreign count and segment start, scatter
+    // bound, as one 32-byte record (16-byte aligned), so that the patch kernel's
+    // copy issue needs one prefetched record instead of dependent global loads
+    const PatchMeta* rec;
 };
 
 // ------------------------------------------------------------------ shared-memory scatter
@@ -259,11 +265,33 @@ constexpr int kForeignAlign = 16;  // foreign segments start at multiples of 16 
 __host__ __device__ inline uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
 
 // A patch's sizes, written by the issuing thread next to its bulk copies.
-struct PatchMeta {
+struct __align__(16) PatchMeta {
     int n_el, o0, nown, nfor, fa;
     float bound;  // PatchView::bound32 of the patch
     int pad0, pad1;
 };
+
+// PatchView::rec from the per-patch offsets and bounds
+__global__ void k_patch_records(PatchView pv, PatchMeta* __restrict__ rec) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pv.n_patches) return;
+    PatchMeta m;
+    m.n_el = pv.pe[p + 1] - pv.pe[p];
+    m.o0 = pv.po[p];
+    m.nown = pv.po[p + 1] - m.o0;
+    m.nfor = pv.pf[p + 1] - pv.pf[p];
+    m.fa = pv.pfa[p];
+    m.bound = pv.bound32[p];
+    m.pad0 = m.pad1 = 0;
+    rec[p] = m;
+}
+
+// 16-byte asynchronous copy global -> shared (cp.async, no bulk); completes at cp_async_wait_all
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // per-buffer bytes of [meta | foreign ids | foreign flags | halo slots (halo == 1)]
 __host__ __device__ inline uint32_t patch_aux_ids(int max_for) {
@@ -396,16 +424,18 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
     // the accumulators start at zero; each flush clears what it reads
     for (int i = threadIdx.x; i < SC::kWords * M; i += blockDim.x) ys[i] = 0;
     __syncthreads();
+    // Thread 0 issues the copies of patch q_j (the block's j-th patch) from its record
+    // in s_rec[j & 1], prefetched by cp.async when q_(j-1) was issued, so that no
+    // issue waits on a global load.
+    __shared__ PatchMeta s_rec[2];
+    auto prefetch_rec = [&](int patch, int slot) {
+        cp_async16(&s_rec[slot], pv.rec + patch);
+        cp_async16(reinterpret_cast<unsigned char*>(&s_rec[slot]) + 16,
+                   reinterpret_cast<const unsigned char*>(pv.rec + patch) + 16);
+        cp_async_commit();
+    };
     // thread 0: the patch's element data, sizes, foreign ids and foreign flags into buffer b
-    auto issue = [&](int patch, int b) {
-        PatchMeta m;
-        m.n_el = pv.pe[patch + 1] - pv.pe[patch];
-        m.o0 = pv.po[patch];
-        m.nown = pv.po[patch + 1] - m.o0;
-        m.nfor = pv.pf[patch + 1] - pv.pf[patch];
-        m.fa = pv.pfa[patch];
-        m.bound = pv.bound32[patch];
-        m.pad0 = m.pad1 = 0;
+    auto issue = [&](const PatchMeta& m, int patch, int b) {
         unsigned char* ab = abuf + (size_t)b * AUX;
         *reinterpret_cast<PatchMeta*>(ab) = m;  // published by the arrive below
         const uint32_t ib = round16((uint32_t)m.nfor * 4u), fb = round16((uint32_t)m.nfor);
@@ -420,9 +450,9 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
         }
     };
     // thread 0: D^-1, r, p_old and flags of the patch's own nodes (single buffer, bar[2])
-    auto issue_own = [&](int patch) {
+    auto issue_own = [&](const PatchMeta& m) {
         constexpr int V = 16 / (int)sizeof(T);  // values per 16 bytes
-        const int o0 = pv.po[patch], o1 = pv.po[patch + 1];
+        const int o0 = m.o0, o1 = m.o0 + m.nown;
         const int a0 = (DPN * o0) & ~(V - 1), nv = ((DPN * o1 + V - 1) & ~(V - 1)) - a0;  // 16-byte aligned
         const int f0 = o0 & ~15, nf = ((o1 + 15) & ~15) - f0;                             // flags, 16-byte aligned
         const uint32_t vb = (uint32_t)nv * (uint32_t)sizeof(T);
@@ -435,9 +465,19 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
         if (nf) bulk_g2s(own_f, pv.flags + f0, (uint32_t)nf, &bar[2]);
     };
     if (threadIdx.x == 0 && blockIdx.x < pv.n_patches) {
-        issue(blockIdx.x, 0);
-        if (OWNB) issue_own(blockIdx.x);
+        const PatchMeta m0 = pv.rec[blockIdx.x];
+        issue(m0, blockIdx.x, 0);
+        if (OWNB) issue_own(m0);
+        if (blockIdx.x + gridDim.x < pv.n_patches) prefetch_rec(blockIdx.x + gridDim.x, 1);
     }
+    // thread 0: patch + gridDim.x (the block's (k+1)-th) into buffer b from its prefetched
+    // record, and the record after it into the slot just read from
+    auto issue_next = [&](int patch, int k, int b) {
+        cp_async_wait_all();
+        const PatchMeta m = s_rec[(k + 1) & 1];
+        issue(m, patch + gridDim.x, b);
+        if (patch + 2 * (int)gridDim.x < pv.n_patches) prefetch_rec(patch + 2 * gridDim.x, k & 1);
+    };
     uint32_t phase = 0;  // bit b = parity of buffer b; bit 2 = parity of the own-node buffer
     // bit b: a copy into buffer b is in flight (tracked by thread 0, which issues them)
     uint32_t pend = blockIdx.x < pv.n_patches ? (OWNB ? 5u : 1u) : 0u;
@@ -447,7 +487,7 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
         const int b = NBUF == 2 ? (k & 1) : 0;
         const bool has_next = patch + (int)gridDim.x < pv.n_patches;
         if (!LATE && NBUF == 2 && threadIdx.x == 0 && has_next) {
-            issue(patch + gridDim.x, b ^ 1);
+            issue_next(patch, k, b ^ 1);
             pend |= 1u << (b ^ 1);
         }
         // The patch's sizes, element data and foreign lists. No block barrier here: a
@@ -567,6 +607,7 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
                 // let copies still in flight land (bounded waits) before the block's shared memory is released
                 for (int q = 0; q < 3; ++q)
                     if ((pend >> q) & 1) mbar_wait(&bar[q], (phase >> q) & 1);
+                cp_async_wait_all();
             }
             return;
         }
@@ -575,11 +616,12 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
         // takes the next patch's slices, during steps 2 and 3.
         if (threadIdx.x == 0 && has_next) {
             if (LATE) {
-                issue(patch + gridDim.x, b ^ 1);
+                issue_next(patch, k, b ^ 1);
                 pend |= 1u << (b ^ 1);
             }
-            if (OWNB) {
-                issue_own(patch + gridDim.x);
+            if (OWNB) {  // the record of patch + gridDim.x is still in its slot
+                cp_async_wait_all();  // single buffer: prefetched by the previous patch's issue
+                issue_own(s_rec[(k + 1) & 1]);
                 pend |= 4u;
             }
         }
@@ -672,7 +714,7 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
         if (!LATE) {
             __syncthreads();
             if (NBUF == 1 && threadIdx.x == 0 && has_next) {
-                issue(patch + gridDim.x, 0);
+                issue_next(patch, k, 0);
                 pend |= 1u;
             }
         }
