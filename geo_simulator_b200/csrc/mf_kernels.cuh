@@ -619,8 +619,11 @@ __global__ void __launch_bounds__(kPatchBS, patch_min_blocks<K, T>())
                 issue_next(patch, k, b ^ 1);
                 pend |= 1u << (b ^ 1);
             }
-            if (OWNB) {  // the record of patch + gridDim.x is still in its slot
-                cp_async_wait_all();  // single buffer: prefetched by the previous patch's issue
+            if (OWNB) {
+                // The record of patch + gridDim.x is in its slot: issue_next of this patch
+                // waited for it (two buffers), or the previous patch's prefetched it (one
+                // buffer). Waiting in the first case would wait for the prefetch just issued.
+                if (NBUF == 1) cp_async_wait_all();
                 issue_own(s_rec[(k + 1) & 1]);
                 pend |= 4u;
             }
