@@ -577,8 +577,15 @@ def csr_vs_matfree(ctx):
     fd = torch.from_numpy(f).to(dev)
     cg = geo.ConjugateGradient().with_tolerance(NOMINAL_TOL).with_max_iterations(20000)
     geo.Assembler.assemble_thermal_stiffness_parallel(mesh, dm, 3.0, ctx)  # warm (inverse map, pattern)
-    t_asm, (Kb, fb) = _device_timed(ctx, lambda: geo.Assembler.apply_dirichlet_bcs(
-        geo.Assembler.assemble_thermal_stiffness_parallel(mesh, dm, 3.0, ctx), fd, dm, ctx))
+    # median of three calls: a single one can pay for the allocator's first mapping of the
+    # CSR arrays (about 0.7 GB) after the 128^3 runs
+    t_asms = []
+    for _ in range(3):
+        Kb = fb = None
+        t, (Kb, fb) = _device_timed(ctx, lambda: geo.Assembler.apply_dirichlet_bcs(
+            geo.Assembler.assemble_thermal_stiffness_parallel(mesh, dm, 3.0, ctx), fd, dm, ctx))
+        t_asms.append(t)
+    t_asm = statistics.median(t_asms)
     cg.solve(Kb, fb)
     t_csr, (x_csr, st_csr) = _device_timed(ctx, lambda: cg.solve(Kb, fb), 2)
     op = geo.ThermalOperator(mesh, dm, 3.0, ctx)
